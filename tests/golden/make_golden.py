@@ -1,0 +1,178 @@
+"""Generate the golden fixtures in this directory from the ASUKA reference.
+
+Runs only where the reference (with its CPU Cython extensions built) is
+importable, e.g.::
+
+    PYTHONPATH=/tmp/asuka_ref OMP_NUM_THREADS=8 python tests/golden/make_golden.py [case ...]
+
+Every fixture is produced by the reference's own public CPU path:
+
+* ``run_hf_df(mol, method='rhf', backend='cpu', df=True, auxbasis='ricd')``
+  (``asuka/frontend/scf.py:1219``) for the SCF energy, orbitals, S, hcore, the
+  DF metric and the whitened factors B;
+* ``asuka.hf.df_scf._df_JK`` (``asuka/hf/df_scf.py:516``) for J and K at the
+  converged density;
+* ``compute_df_gradient_contributions_analytic_packed_bases(backend='cpu')``
+  (``asuka/integrals/grad.py:114``) for the DF two-electron gradient at fixed
+  density, with ``bar_L[Q] = rho_Q D - 1/2 D B_Q D``;
+* ``_eri_rys_cpu.eri_rys_tile_cart_sp_batch_cy`` for single (ab|P) and (P|Q)
+  tiles of every angular class of H2O/ma-QZVP;
+* ``_eri_rys_cpu.rys_roots_weights_cy`` for reference roots/weights.
+
+Geometries come from ``asuka_b200.geometry`` so that tests rebuild identical
+inputs without the reference.
+"""
+
+from __future__ import annotations
+
+import os
+import sys
+import time
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.abspath(os.path.join(HERE, "..", "..")))
+
+from asuka_b200 import geometry as geo  # noqa: E402
+
+
+def _ref_mol(mol):
+    from asuka.frontend.molecule import Molecule
+
+    return Molecule.from_atoms([(el, xyz) for el, xyz in mol.atoms_bohr], unit="Bohr", basis=mol.basis, cart=True)
+
+
+def _tril_pack(X):
+    nao = X.shape[0]
+    i, j = np.tril_indices(nao)
+    return X[i, j]
+
+
+def scf_case(name: str, mol, with_grad: bool = True) -> None:
+    from asuka.frontend.scf import run_hf_df
+    from asuka.hf.df_scf import _df_JK
+    from asuka.integrals.grad import compute_df_gradient_contributions_analytic_packed_bases
+
+    rmol = _ref_mol(mol)
+    prof: dict = {}
+    t0 = time.perf_counter()
+    res = run_hf_df(rmol, method="rhf", backend="cpu", df=True, auxbasis="ricd", conv_tol=1e-10, profile=prof)
+    t_scf = time.perf_counter() - t0
+    B = np.asarray(res.df_B)
+    L = np.asarray(res.df_L)
+    nao, _, naux = B.shape
+    C = np.asarray(res.mo_coeff)
+    occ = np.asarray(res.mo_occ)
+    D = (C * occ[None, :]) @ C.T
+    J, K = _df_JK(B, D, want_J=True, want_K=True)
+    rho = np.einsum("mnQ,mn->Q", B, D)
+    E2 = 0.5 * float(np.sum(D * J)) - 0.25 * float(np.sum(D * K))
+    X = np.einsum("mnP,QP->mnQ", B, L)  # unwhitened (mu nu|P) = B L^T
+    out = dict(
+        elements=np.array(mol.elements),
+        coords_bohr=mol.coords_bohr,
+        basis=np.array(mol.basis),
+        S=np.asarray(res.int1e.S),
+        hcore=np.asarray(res.int1e.hcore),
+        e_nuc=np.array(res.e_nuc),
+        e_tot=np.array(res.e_tot),
+        niter=np.array(res.scf.niter),
+        mo_energy=np.asarray(res.mo_energy),
+        mo_coeff=C,
+        mo_occ=occ,
+        D=D,
+        J=np.asarray(J),
+        K=np.asarray(K),
+        E2=np.array(E2),
+        V=L @ L.T,
+        X_tril=np.stack([_tril_pack(X[:, :, P]) for P in range(naux)], axis=0),  # (naux, ntri)
+        t_scf_s=np.array(t_scf),
+    )
+    if with_grad:
+        barL = rho[:, None, None] * D[None, :, :] - 0.5 * np.einsum("mk,knQ,nl->Qml", D, B, D)
+        t0 = time.perf_counter()
+        g2 = compute_df_gradient_contributions_analytic_packed_bases(
+            res.ao_basis, res.aux_basis, atom_coords_bohr=mol.coords_bohr, B_ao=B, bar_L_ao=barL, L_chol=L,
+            backend="cpu")
+        out["grad_2e"] = np.asarray(g2)
+        out["t_grad_s"] = np.array(time.perf_counter() - t0)
+    np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **out)
+    print(f"{name}: nao={nao} naux={naux} E={res.e_tot:.12f} iters={res.scf.niter} t_scf={t_scf:.1f}s", flush=True)
+
+
+def tiles_case(name: str, mol) -> None:
+    """One (ab|P) tile per (la, lb, lP) class and one (P|Q) tile per (lP, lQ) class."""
+    from asuka.cueri import _eri_rys_cpu as ext
+    from asuka.cueri.pair_tables_cpu import build_pair_tables_cpu
+    from asuka.frontend.one_electron import build_ao_basis_cart
+    from asuka.frontend._scf_build import build_aux_basis_cart
+    from asuka.integrals.cueri_df_cpu import _build_df_combined_basis_and_shell_pairs
+
+    rmol = _ref_mol(mol)
+    ao, _ = build_ao_basis_cart(rmol, basis=mol.basis, expand_contractions=True)
+    aux, _ = build_aux_basis_cart(rmol, basis_in=mol.basis, auxbasis="ricd", expand_contractions=True, ao_basis=ao)
+    ball, sp, nsp_ao, nsh_ao, nsh_aux = _build_df_combined_basis_and_shell_pairs(ao, aux)
+    pt = build_pair_tables_cpu(ball, sp, threads=0)
+    args = [np.asarray(ball.shell_cxyz), np.asarray(ball.shell_l), sp.sp_A, sp.sp_B, sp.sp_pair_start, sp.sp_npair,
+            pt.pair_eta, pt.pair_Px, pt.pair_Py, pt.pair_Pz, pt.pair_cK]
+    ao_l = np.asarray(ao.shell_l)
+    aux_l = np.asarray(aux.shell_l)
+    trip, vals3 = [], []
+    seen = set()
+    for spAB in range(nsp_ao):
+        A, B = int(sp.sp_A[spAB]), int(sp.sp_B[spAB])
+        for Pc in range(nsh_aux):
+            key = (int(ao_l[A]), int(ao_l[B]), int(aux_l[Pc]))
+            if key in seen:
+                continue
+            seen.add(key)
+            t = ext.eri_rys_tile_cart_sp_batch_cy(*args, int(spAB), np.array([nsp_ao + Pc], dtype=np.int32), 0)
+            trip.append((A, B, Pc))
+            vals3.append(np.asarray(t[0]).ravel())
+    pairs, vals2 = [], []
+    seen = set()
+    for P in range(nsh_aux):
+        for Q in range(P + 1):
+            key = (int(aux_l[P]), int(aux_l[Q]))
+            if key in seen:
+                continue
+            seen.add(key)
+            t = ext.eri_rys_tile_cart_sp_batch_cy(*args, int(nsp_ao + P), np.array([nsp_ao + Q], dtype=np.int32), 0)
+            pairs.append((P, Q))
+            vals2.append(np.asarray(t[0]).ravel())
+    np.savez_compressed(
+        os.path.join(HERE, f"{name}.npz"),
+        elements=np.array(mol.elements), coords_bohr=mol.coords_bohr, basis=np.array(mol.basis),
+        trip=np.array(trip, dtype=np.int32), tiles3=np.concatenate(vals3), len3=np.array([v.size for v in vals3]),
+        pairs=np.array(pairs, dtype=np.int32), tiles2=np.concatenate(vals2), len2=np.array([v.size for v in vals2]))
+    print(f"{name}: {len(trip)} (ab|P) classes, {len(pairs)} (P|Q) classes", flush=True)
+
+
+def roots_case() -> None:
+    from asuka.cueri import _eri_rys_cpu as ext
+
+    Ts = np.concatenate([[0.0, 1e-10, 1e-3], np.linspace(0.05, 4.95, 12), [5.0, 5.05], np.geomspace(5.5, 500.0, 14)])
+    r = np.zeros((10, Ts.size, 10))
+    w = np.zeros_like(r)
+    for n in range(1, 11):
+        for i, T in enumerate(Ts):
+            rr, ww = ext.rys_roots_weights_cy(n, float(T))
+            r[n - 1, i, :n] = rr
+            w[n - 1, i, :n] = ww
+    np.savez_compressed(os.path.join(HERE, "ref_roots.npz"), T=Ts, roots=r, weights=w)
+    print("ref_roots: done", flush=True)
+
+
+CASES = {
+    "n2_masvp": lambda: scf_case("n2_masvp", geo.n2("ma-svp")),
+    "h2o_masvp": lambda: scf_case("h2o_masvp", geo.water("ma-svp")),
+    "h2o_matzvp": lambda: scf_case("h2o_matzvp", geo.water("ma-tzvp")),
+    "tiles_h2o_maqzvp": lambda: tiles_case("tiles_h2o_maqzvp", geo.water("ma-qzvp")),
+    "ref_roots": roots_case,
+}
+
+if __name__ == "__main__":
+    todo = sys.argv[1:] or list(CASES)
+    for c in todo:
+        CASES[c]()
