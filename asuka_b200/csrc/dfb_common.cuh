@@ -1,0 +1,61 @@
+// Shared device helpers for the DF two-electron kernels (sm_100a).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#define DFB_LMAX 8                                 // highest shell l on either side
+#define DFB_NROOTS_MAX 10                          // (4+4+8+1)/2+1 = 9 needed; table holds 10
+#define DFB_WARPS_PER_BLOCK 4
+
+namespace dfb {
+
+__host__ __device__ __forceinline__ int ncart(int l) { return (l + 1) * (l + 2) / 2; }
+
+// number of Cartesian components over all l < L (tetrahedral numbers)
+__host__ __device__ __forceinline__ int ncart_below(int L) { return L * (L + 1) * (L + 2) / 6; }
+
+// position of (ex, ey, ez=l-ex-ey) inside shell l, x-major order (for x=l..0, for y=l-x..0)
+__host__ __device__ __forceinline__ int cart_index(int ex, int ey, int l) {
+    return ((l - ex) * (l - ex + 1)) / 2 + (l - ex - ey);
+}
+
+// Rys root/weight table: per root count n, NINT unit intervals in T, 2n rows
+// (n nodes then n weights), DEG+1 power-basis coefficients in u = 2(T-k)-1.
+struct RysTable {
+    const double* coef;   // concatenated over n = 1..nmax
+    const double* herm;   // per n: s_i^2 (n) then W_i (n), concatenated
+    int offs[DFB_NROOTS_MAX + 1];   // coefficient offset of root count n
+    int hoff[DFB_NROOTS_MAX + 1];   // hermite offset of root count n
+    int nmax, nint, deg;
+    double tmax;
+};
+
+// Nodes x_i (in t^2) and weights w_i (sum w_i = F_0(T)) of the n-point Rys rule.
+__device__ __forceinline__ void rys_eval(const RysTable& tab, int n, double T, double* x, double* w) {
+    if (T >= tab.tmax) {
+        const double* h = tab.herm + tab.hoff[n];
+        const double inv = 1.0 / T;
+        const double rs = rsqrt(T);
+        for (int i = 0; i < n; ++i) {
+            x[i] = __ldg(h + i) * inv;
+            w[i] = __ldg(h + n + i) * rs;
+        }
+        return;
+    }
+    int k = (int)T;
+    if (k > tab.nint - 1) k = tab.nint - 1;
+    const double u = 2.0 * (T - (double)k) - 1.0;
+    const int stride = tab.deg + 1;
+    const double* c = tab.coef + tab.offs[n] + (size_t)k * (2 * n) * stride;
+    for (int r = 0; r < 2 * n; ++r) {
+        const double* cr = c + r * stride;
+        double acc = __ldg(cr + tab.deg);
+        for (int d = tab.deg - 1; d >= 0; --d) acc = fma(acc, u, __ldg(cr + d));
+        if (r < n)
+            x[r] = acc;
+        else
+            w[r - n] = acc;
+    }
+}
+
+}  // namespace dfb

@@ -1,0 +1,9 @@
+// Host-side error reporting shared by the libdfb translation units.
+#pragma once
+#include <cuda_runtime.h>
+
+namespace dfb {
+void clear_error();
+int set_error(int code, const char* fmt, ...);
+int set_cuda_error(const char* what, cudaError_t e);
+}  // namespace dfb

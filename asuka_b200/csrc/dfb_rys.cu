@@ -1,0 +1,640 @@
+// Rys-quadrature DF integrals and their derivative contraction on sm_100a.
+//
+// One warp owns one task (an AB shell pair -- or an aux self-pair for the
+// metric -- times one aux shell C) at a time and walks every task of the
+// launch's angular class in a persistent loop:
+//
+//   1. the 32 lanes take 32 primitive triplets at once and evaluate T, the
+//      Rys nodes/weights (table lookup, FP64) and the prefactor;
+//   2. for each primitive triplet, lanes (root, direction) build the 2D
+//      recurrence tables G[a][b] (a <= la+lb(+1), b <= lc) in shared memory,
+//      the x table pre-scaled by weight*prefactor;
+//   3. every lane accumulates its share of the contracted intermediate
+//      (e 0 | f) = sum Gx Gy Gz  (la <= |e| <= la+lb, f in shell c) in registers;
+//   4. after all primitives the horizontal recurrence (e 0|f) -> (a b|f) runs
+//      once per contracted task, and the tile goes straight to its final place
+//      (3c tensor both (mu,nu) orders, or both halves of the metric).
+//
+// The derivative variant accumulates, per AO primitive pair, the plain sum U
+// and the exponent-weighted sums 2a*S, 2b*S over |e| up to la+lb+1, then
+// contracts d/dA = 2a (a+1) - a_x (a-1) and d/dB = 2b [(a+1,b) + AB (a,b)] -
+// b_x (a,b-1) against the adjoint tile; d/dC follows from translational
+// invariance.  Per-block partial gradients live in shared memory.
+//
+// Mathematics restated from the reference (asuka/cueri/_eri_rys_cpu.pyx
+// :690-718 recurrences, :802-817 horizontal shift, :2650-2957 derivative
+// contraction); roots come from a tabulated fit instead of the reference's
+// per-call moment solver.
+
+#include <stdio.h>
+#include <string.h>
+
+#include "../../include/dfb.h"
+#include "dfb_common.cuh"
+#include "dfb_internal.h"
+
+namespace dfb {
+
+static const double kTwoPi52 = 2.0 * 3.141592653589793238462643383279502884 * 3.141592653589793238462643383279502884 *
+                               1.772453850905516027298167483341145182;
+
+struct ClassInfo {
+    int la, lb, lc;
+    int nr;          // Rys roots
+    int nmax, mmax;  // G table extents
+    int lmin, lmax;  // |e| range of the contracted intermediate
+    int ne, nf, nef;
+    int na, nb, nc;
+    int gt;          // (nmax+1)*(mmax+1)
+    int item;        // doubles per primitive-triplet record
+};
+
+static ClassInfo make_class(int la, int lb, int lc, bool deriv) {
+    ClassInfo c;
+    c.la = la;
+    c.lb = lb;
+    c.lc = lc;
+    c.nr = (la + lb + lc + (deriv ? 1 : 0)) / 2 + 1;
+    c.nmax = la + lb + (deriv ? 1 : 0);
+    c.mmax = lc;
+    c.lmin = deriv ? (la > 0 ? la - 1 : 0) : la;
+    c.lmax = c.nmax;
+    c.ne = ncart_below(c.lmax + 1) - ncart_below(c.lmin);
+    c.nf = ncart(lc);
+    c.nef = c.ne * c.nf;
+    c.na = ncart(la);
+    c.nb = ncart(lb);
+    c.nc = ncart(lc);
+    c.gt = (c.nmax + 1) * (c.mmax + 1);
+    c.item = 8 + 2 * c.nr;
+    return c;
+}
+
+__device__ __forceinline__ void decode_cart(int l, int idx, int& x, int& y, int& z) {
+    int xx = l;
+    while (idx > l - xx) {
+        idx -= (l - xx + 1);
+        --xx;
+    }
+    x = xx;
+    y = l - xx - idx;
+    z = idx;
+}
+
+__device__ __forceinline__ void decode_e(const ClassInfo& ci, int e, int& x, int& y, int& z) {
+    int L = ci.lmin;
+    while (e >= ncart(L)) {
+        e -= ncart(L);
+        ++L;
+    }
+    decode_cart(L, e, x, y, z);
+}
+
+__device__ __forceinline__ int e_index(const ClassInfo& ci, int x, int y, int z) {
+    const int L = x + y + z;
+    return ncart_below(L) - ncart_below(ci.lmin) + cart_index(x, y, L);
+}
+
+__constant__ double c_binom[DFB_LMAX + 2][DFB_LMAX + 2];
+
+// (a b | f) = sum_k C(b,k) AB^(b-k) (a+k 0 | f), per direction, from E[e*nf + f].
+__device__ __forceinline__ double hrr(const ClassInfo& ci, const double* E, int ax, int ay, int az, int bx, int by,
+                                      int bz, int f, const double* AB) {
+    double sum = 0.0;
+    double px = 1.0;
+    for (int kx = bx; kx >= 0; --kx) {
+        const double cx = c_binom[bx][kx] * px;
+        double py = 1.0;
+        for (int ky = by; ky >= 0; --ky) {
+            const double cxy = cx * c_binom[by][ky] * py;
+            double pz = 1.0;
+            for (int kz = bz; kz >= 0; --kz) {
+                const double c = cxy * c_binom[bz][kz] * pz;
+                sum += c * E[e_index(ci, ax + kx, ay + ky, az + kz) * ci.nf + f];
+                pz *= AB[2];
+            }
+            py *= AB[1];
+        }
+        px *= AB[0];
+    }
+    return sum;
+}
+
+__device__ __forceinline__ void build_G(double* G, int nmax, int mmax, double g00, double C, double Cp, double B0,
+                                        double B1, double B1p) {
+    const int M = mmax + 1;
+    G[0] = g00;
+    if (nmax > 0) G[M] = C * g00;
+    if (mmax > 0) G[1] = Cp * g00;
+    for (int a = 2; a <= nmax; ++a) G[a * M] = B1 * (double)(a - 1) * G[(a - 2) * M] + C * G[(a - 1) * M];
+    for (int b = 2; b <= mmax; ++b) G[b] = B1p * (double)(b - 1) * G[b - 2] + Cp * G[b - 1];
+    if (nmax == 0 || mmax == 0) return;
+    for (int a = 1; a <= nmax; ++a) {
+        G[a * M + 1] = (double)a * B0 * G[(a - 1) * M] + Cp * G[a * M];
+        for (int b = 2; b <= mmax; ++b)
+            G[a * M + b] = B1p * (double)(b - 1) * G[a * M + b - 2] + (double)a * B0 * G[(a - 1) * M + b - 1] +
+                           Cp * G[a * M + b - 1];
+    }
+}
+
+template <int KB, bool DERIV>
+__global__ void __launch_bounds__(DFB_WARPS_PER_BLOCK * 32)
+    k_rys(ClassInfo ci, dfb_pair_side_t ps, dfb_aux_side_t ax, const int* __restrict__ task_pair,
+          const int* __restrict__ task_aux, long ntask, long naux_grid, int mode, double* __restrict__ out, long sP,
+          long sM, long sN, const double* __restrict__ bar, long sbP, long sbM, long sbN, double* __restrict__ grad, int natm,
+          int smem_grad, double* __restrict__ scratch, long slot, RysTable tab) {
+    extern __shared__ double smem[];
+    const int lane = threadIdx.x & 31;
+    const int wib = threadIdx.x >> 5;
+    double* sgrad = smem;
+    const int ngrad = (DERIV && smem_grad) ? natm * 3 : 0;
+    const int per_warp = 32 * ci.item + ci.nr * 3 * ci.gt;
+    double* items = smem + ngrad + wib * per_warp;
+    double* gtab = items + 32 * ci.item;
+    const long gwarp = (long)blockIdx.x * DFB_WARPS_PER_BLOCK + wib;
+    const long nwarps = (long)gridDim.x * DFB_WARPS_PER_BLOCK;
+    double* E = scratch + gwarp * slot;  // U | WA | WB for DERIV, else E
+
+    if (DERIV && smem_grad) {
+        for (int i = threadIdx.x; i < ngrad; i += blockDim.x) sgrad[i] = 0.0;
+        __syncthreads();
+    }
+
+    // Elements (e, f) of the contracted intermediate are split over the lanes,
+    // KB per lane per chunk; large classes loop over several chunks, re-running
+    // the primitive loop for each (their tasks are few).
+    const int chunk_elems = 32 * KB;
+    const int nchunk = (ci.nef + chunk_elems - 1) / chunk_elems;
+    const int M = ci.mmax + 1;
+    int off[KB];
+    auto make_offsets = [&](int cbase) {
+#pragma unroll
+        for (int k = 0; k < KB; ++k) {
+            const int t = cbase + lane + 32 * k;
+            off[k] = -1;
+            if (t < ci.nef) {
+                const int e = t / ci.nf, f = t - (t / ci.nf) * ci.nf;
+                int ex, ey, ez, fx, fy, fz;
+                decode_e(ci, e, ex, ey, ez);
+                decode_cart(ci.lc, f, fx, fy, fz);
+                off[k] = (ex * M + fx) | ((ey * M + fy) << 10) | ((ez * M + fz) << 20);
+            }
+        }
+    };
+    if (nchunk == 1) make_offsets(0);
+
+    for (long task = gwarp; task < ntask; task += nwarps) {
+        const long tp = naux_grid > 0 ? task / naux_grid : task;
+        const long ta = naux_grid > 0 ? task - tp * naux_grid : task;
+        const int pair = task_pair[tp];
+        const int C = task_aux[ta];
+        const int shA = ps.shA[pair];
+        const int shB = ps.b_dummy ? -1 : ps.shB[pair];
+        double A[3], AB[3], Cc[3];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            A[d] = ps.cxyz[3 * shA + d];
+            const double Bd = ps.b_dummy ? 0.0 : ps.cxyz[3 * shB + d];
+            AB[d] = A[d] - Bd;
+            Cc[d] = ax.cxyz[3 * C + d];
+        }
+        const int p0 = ps.pstart[pair];
+        const int nprimAB = ps.npair[pair];
+        const int c0 = ax.pstart[C];
+        const int nprimC = ax.nprim[C];
+        const long nitems = (long)nprimAB * nprimC;
+
+        if (DERIV) {
+            for (int t = lane; t < 3 * ci.nef; t += 32) E[t] = 0.0;
+        }
+
+        for (int ch = 0; ch < nchunk; ++ch) {
+            const int cbase = ch * chunk_elems;
+            if (nchunk > 1) make_offsets(cbase);
+            double acc[KB];
+#pragma unroll
+            for (int k = 0; k < KB; ++k) acc[k] = 0.0;
+
+            for (long base = 0; base < nitems; base += 32) {
+                const long j = base + lane;
+                if (j < nitems) {
+                    const int iab = (int)(j / nprimC);
+                    const int ic = (int)(j - (long)iab * nprimC);
+                    const double p = ps.eta[p0 + iab];
+                    const double Pp[3] = {ps.Px[p0 + iab], ps.Py[p0 + iab], ps.Pz[p0 + iab]};
+                    const double q = ax.pexp[c0 + ic];
+                    const double inv = 1.0 / (p + q);
+                    double PQ2 = 0.0;
+                    double* it = items + lane * ci.item;
+                    it[0] = p;
+                    it[1] = q;
+#pragma unroll
+                    for (int d = 0; d < 3; ++d) {
+                        const double cp = Cc[d] - Pp[d];
+                        PQ2 += cp * cp;
+                        it[2 + d] = Pp[d] - A[d];
+                        it[5 + d] = cp;
+                    }
+                    const double T = p * q * inv * PQ2;
+                    const double pref = kTwoPi52 / (p * q * sqrt(p + q)) * ps.cK[p0 + iab] * ax.pcoef[c0 + ic];
+                    double xr[DFB_NROOTS_MAX], wr[DFB_NROOTS_MAX];
+                    rys_eval(tab, ci.nr, T, xr, wr);
+                    for (int u = 0; u < ci.nr; ++u) {
+                        it[8 + u] = xr[u];
+                        it[8 + ci.nr + u] = pref * wr[u];
+                    }
+                }
+                __syncwarp();
+                const int nb = (int)((nitems - base) < 32 ? (nitems - base) : 32);
+                for (int jj = 0; jj < nb; ++jj) {
+                    const double* it = items + jj * ci.item;
+                    if (lane < ci.nr * 3) {
+                        const int u = lane / 3, d = lane - 3 * (lane / 3);
+                        const double p = it[0], q = it[1];
+                        const double inv = 1.0 / (p + q);
+                        const double x = it[8 + u];
+                        const double B0 = x * 0.5 * inv;
+                        const double B1 = (1.0 - x) * 0.5 / p + B0;
+                        const double B1p = (1.0 - x) * 0.5 / q + B0;
+                        const double Cd = it[2 + d] + (q * inv) * x * it[5 + d];
+                        const double Cpd = -(p * inv) * x * it[5 + d];
+                        const double g00 = (d == 0) ? it[8 + ci.nr + u] : 1.0;
+                        build_G(gtab + (u * 3 + d) * ci.gt, ci.nmax, ci.mmax, g00, Cd, Cpd, B0, B1, B1p);
+                    }
+                    __syncwarp();
+#pragma unroll
+                    for (int k = 0; k < KB; ++k) {
+                        if (off[k] >= 0) {
+                            const int ox = off[k] & 1023, oy = (off[k] >> 10) & 1023, oz = off[k] >> 20;
+                            double v = 0.0;
+                            for (int u = 0; u < ci.nr; ++u) {
+                                const double* g = gtab + u * 3 * ci.gt;
+                                v = fma(g[ox] * g[ci.gt + oy], g[2 * ci.gt + oz], v);
+                            }
+                            acc[k] += v;
+                        }
+                    }
+                    if (DERIV) {
+                        const long gidx = base + jj;
+                        if ((gidx + 1) % nprimC == 0) {
+                            const int iab = (int)(gidx / nprimC);
+                            const double a2 = 2.0 * ps.ea[p0 + iab];
+                            const double b2 = 2.0 * ps.eb[p0 + iab];
+#pragma unroll
+                            for (int k = 0; k < KB; ++k) {
+                                const int t = cbase + lane + 32 * k;
+                                if (off[k] >= 0) {
+                                    E[t] += acc[k];
+                                    E[ci.nef + t] += a2 * acc[k];
+                                    E[2 * ci.nef + t] += b2 * acc[k];
+                                    acc[k] = 0.0;
+                                }
+                            }
+                        }
+                    }
+                    __syncwarp();
+                }
+            }
+            if (!DERIV) {
+#pragma unroll
+                for (int k = 0; k < KB; ++k) {
+                    if (off[k] >= 0) E[cbase + lane + 32 * k] = acc[k];
+                }
+            }
+        }
+        __syncwarp();
+
+        const int aoA = ps.aostart[shA];
+        const int aoB = ps.b_dummy ? 0 : ps.aostart[shB];
+        const int aoC = ax.aostart[C];
+        const int ntile = ci.na * ci.nb * ci.nc;
+        double gA[3] = {0.0, 0.0, 0.0}, gB[3] = {0.0, 0.0, 0.0};
+        for (int idx = lane; idx < ntile; idx += 32) {
+            const int ic = idx % ci.nc;
+            const int iab = idx / ci.nc;
+            const int ib = iab % ci.nb;
+            const int ia = iab / ci.nb;
+            int a[3], b[3];
+            decode_cart(ci.la, ia, a[0], a[1], a[2]);
+            decode_cart(ci.lb, ib, b[0], b[1], b[2]);
+            if (!DERIV) {
+                const double v = hrr(ci, E, a[0], a[1], a[2], b[0], b[1], b[2], ic, AB);
+                if (mode == 0) {
+                    const long P = aoC + ic, mu = aoA + ia, nu = aoB + ib;
+                    out[P * sP + mu * sM + nu * sN] = v;
+                    out[P * sP + nu * sM + mu * sN] = v;
+                } else {
+                    const long Pa = aoA + ia, Qc = aoC + ic;
+                    out[Qc * sP + Pa * sM] = v;
+                    out[Pa * sP + Qc * sM] = v;
+                }
+            } else {
+                double gam;
+                if (mode == 0) {
+                    gam = bar[(long)(aoC + ic) * sbP + (long)(aoA + ia) * sbM + (long)(aoB + ib) * sbN];
+                } else {
+                    gam = bar[(long)(aoA + ia) * sbP + (long)(aoC + ic) * sbM];
+                }
+                if (gam != 0.0) {
+                    const double* U = E;
+                    const double* WA = E + ci.nef;
+                    const double* WB = E + 2 * ci.nef;
+#pragma unroll
+                    for (int d = 0; d < 3; ++d) {
+                        int ap[3] = {a[0], a[1], a[2]};
+                        ap[d] += 1;
+                        double dA = hrr(ci, WA, ap[0], ap[1], ap[2], b[0], b[1], b[2], ic, AB);
+                        if (a[d] > 0) {
+                            int am[3] = {a[0], a[1], a[2]};
+                            am[d] -= 1;
+                            dA -= (double)a[d] * hrr(ci, U, am[0], am[1], am[2], b[0], b[1], b[2], ic, AB);
+                        }
+                        gA[d] += gam * dA;
+                        if (!ps.b_dummy) {
+                            double dB = hrr(ci, WB, ap[0], ap[1], ap[2], b[0], b[1], b[2], ic, AB) +
+                                        AB[d] * hrr(ci, WB, a[0], a[1], a[2], b[0], b[1], b[2], ic, AB);
+                            if (b[d] > 0) {
+                                int bm[3] = {b[0], b[1], b[2]};
+                                bm[d] -= 1;
+                                dB -= (double)b[d] * hrr(ci, U, a[0], a[1], a[2], bm[0], bm[1], bm[2], ic, AB);
+                            }
+                            gB[d] += gam * dB;
+                        }
+                    }
+                }
+            }
+        }
+        if (DERIV) {
+#pragma unroll
+            for (int d = 0; d < 3; ++d) {
+                for (int s = 16; s > 0; s >>= 1) {
+                    gA[d] += __shfl_xor_sync(0xffffffffu, gA[d], s);
+                    gB[d] += __shfl_xor_sync(0xffffffffu, gB[d], s);
+                }
+            }
+            if (lane == 0) {
+                const bool offdiag = (mode == 0) ? (shA != shB) : (shA != C);
+                const double fac = offdiag ? 2.0 : 1.0;
+                const int atA = ps.atom[shA];
+                const int atB = ps.b_dummy ? -1 : ps.atom[shB];
+                const int atC = ax.atom[C];
+                double* G = smem_grad ? sgrad : grad;
+                for (int d = 0; d < 3; ++d) {
+                    const double vA = fac * gA[d], vB = fac * gB[d];
+                    atomicAdd(G + 3 * atA + d, vA);
+                    if (atB >= 0) atomicAdd(G + 3 * atB + d, vB);
+                    atomicAdd(G + 3 * atC + d, -(vA + vB));
+                }
+            }
+        }
+        __syncwarp();
+    }
+
+    if (DERIV && smem_grad) {
+        __syncthreads();
+        for (int i = threadIdx.x; i < ngrad; i += blockDim.x)
+            if (sgrad[i] != 0.0) atomicAdd(grad + i, sgrad[i]);
+    }
+}
+
+__global__ void k_pair_tables(const double* __restrict__ cxyz, const int* __restrict__ spstart_sh,
+                              const int* __restrict__ nprim_sh, const double* __restrict__ pexp,
+                              const double* __restrict__ pcoef, const int* __restrict__ sp_A,
+                              const int* __restrict__ sp_B, const int* __restrict__ sp_pstart,
+                              const int* __restrict__ pp_sp, long npp, int b_dummy, double* eta, double* Px,
+                              double* Py, double* Pz, double* cK, double* ea, double* eb) {
+    const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= npp) return;
+    const int sp = pp_sp[i];
+    const int A = sp_A[sp];
+    const int local = (int)(i - sp_pstart[sp]);
+    if (b_dummy) {
+        const double a = pexp[spstart_sh[A] + local];
+        eta[i] = a;
+        Px[i] = cxyz[3 * A + 0];
+        Py[i] = cxyz[3 * A + 1];
+        Pz[i] = cxyz[3 * A + 2];
+        cK[i] = pcoef[spstart_sh[A] + local];
+        ea[i] = a;
+        eb[i] = 0.0;
+        return;
+    }
+    const int B = sp_B[sp];
+    const int nB = nprim_sh[B];
+    const int ia = local / nB, ib = local - (local / nB) * nB;
+    const double a = pexp[spstart_sh[A] + ia], b = pexp[spstart_sh[B] + ib];
+    const double ca = pcoef[spstart_sh[A] + ia], cb = pcoef[spstart_sh[B] + ib];
+    const double p = a + b, inv = 1.0 / p, mu = a * b * inv;
+    double AB2 = 0.0;
+    double P[3];
+    for (int d = 0; d < 3; ++d) {
+        const double Ad = cxyz[3 * A + d], Bd = cxyz[3 * B + d];
+        AB2 += (Ad - Bd) * (Ad - Bd);
+        P[d] = (a * Ad + b * Bd) * inv;
+    }
+    eta[i] = p;
+    Px[i] = P[0];
+    Py[i] = P[1];
+    Pz[i] = P[2];
+    cK[i] = (ca * cb) * exp(-mu * AB2);
+    ea[i] = a;
+    eb[i] = b;
+}
+
+// ---------------------------------------------------------------- host side
+
+struct DeviceTable {
+    bool ready = false;
+    double* coef = nullptr;
+    double* herm = nullptr;
+    RysTable tab;
+};
+static DeviceTable g_tables[64];
+static bool g_binom_ready[64];
+
+static int current_device() {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    return dev;
+}
+
+template <int KB, bool DERIV>
+static int launch_rys(const ClassInfo& ci, const dfb_pair_side_t* ps, const dfb_aux_side_t* ax,
+                      const int* task_pair, const int* task_aux, long ntask, long naux_grid, int mode, double* out,
+                      long sP, long sM, long sN, const double* bar, long sbP, long sbM, long sbN, double* grad, int natm,
+                      double* scratch, long scratch_doubles, cudaStream_t st, int query_only, long* need) {
+    const int dev = current_device();
+    const int smem_grad = (DERIV && natm * 3 <= 4096) ? 1 : 0;
+    const size_t smem =
+        sizeof(double) * ((DERIV && smem_grad ? natm * 3 : 0) +
+                          (size_t)DFB_WARPS_PER_BLOCK * (32 * ci.item + ci.nr * 3 * ci.gt));
+    auto kern = k_rys<KB, DERIV>;
+    if (smem > 48 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return set_cuda_error("cudaFuncSetAttribute", e);
+    }
+    // The persistent grid (and so the scratch size) is sized from the occupancy
+    // without the optional per-block gradient buffer, so that the scratch
+    // requirement does not depend on the atom count.
+    const size_t smem_base = sizeof(double) * ((size_t)DFB_WARPS_PER_BLOCK * (32 * ci.item + ci.nr * 3 * ci.gt));
+    if (smem_base > 48 * 1024 && smem <= 48 * 1024) {
+        cudaError_t e0 = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_base);
+        if (e0 != cudaSuccess) return set_cuda_error("cudaFuncSetAttribute", e0);
+    }
+    int occ = 0;
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, DFB_WARPS_PER_BLOCK * 32, smem_base);
+    if (e != cudaSuccess) return set_cuda_error("occupancy", e);
+    if (occ < 1) return set_error(DFB_ERR_UNSUPPORTED, "class (%d,%d,%d) does not fit on an SM", ci.la, ci.lb, ci.lc);
+    int nsm = 0;
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    long blocks_needed = (ntask + DFB_WARPS_PER_BLOCK - 1) / DFB_WARPS_PER_BLOCK;
+    long blocks = (long)occ * nsm;
+    if (blocks > blocks_needed) blocks = blocks_needed;
+    if (blocks < 1) blocks = 1;
+    const long slot = (DERIV ? 3L : 1L) * ci.nef;
+    const long required = blocks * DFB_WARPS_PER_BLOCK * slot;
+    if (query_only) {
+        *need = required;
+        return DFB_OK;
+    }
+    if (ntask == 0) return DFB_OK;
+    if (scratch == nullptr || scratch_doubles < required)
+        return set_error(DFB_ERR_INVALID, "scratch too small: need %ld doubles, got %ld", required, scratch_doubles);
+    kern<<<(unsigned)blocks, DFB_WARPS_PER_BLOCK * 32, smem, st>>>(
+        ci, *ps, *ax, task_pair, task_aux, ntask, naux_grid, mode, out, sP, sM, sN, bar, sbP, sbM, sbN, grad, natm, smem_grad,
+        scratch, slot, g_tables[dev].tab);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return set_cuda_error("k_rys launch", e);
+    return DFB_OK;
+}
+
+template <bool DERIV>
+static int dispatch_rys(int la, int lb, int lc, const dfb_pair_side_t* ps, const dfb_aux_side_t* ax,
+                        const int* task_pair, const int* task_aux, long ntask, long naux_grid, int mode, double* out,
+                        long sP, long sM, long sN, const double* bar, long sbP, long sbM, long sbN, double* grad, int natm,
+                        double* scratch, long scratch_doubles, cudaStream_t st, int query_only, long* need) {
+    if (la < 0 || lb < 0 || lc < 0 || la > DFB_LMAX || lb > DFB_LMAX || lc > DFB_LMAX)
+        return set_error(DFB_ERR_UNSUPPORTED, "angular momentum out of range (la=%d lb=%d lc=%d, max %d)", la, lb, lc,
+                         DFB_LMAX);
+    if (lb > la) return set_error(DFB_ERR_INVALID, "pairs must be l-ordered (la >= lb)");
+    const ClassInfo ci = make_class(la, lb, lc, DERIV);
+    if (ci.nr > DFB_NROOTS_MAX) return set_error(DFB_ERR_UNSUPPORTED, "too many Rys roots (%d)", ci.nr);
+    const int dev = current_device();
+    if (!query_only && !g_tables[dev].ready)
+        return set_error(DFB_ERR_NOT_INITIALISED, "Rys table not uploaded on device %d", dev);
+    if (!g_binom_ready[dev]) {
+        double h[DFB_LMAX + 2][DFB_LMAX + 2];
+        for (int n = 0; n < DFB_LMAX + 2; ++n)
+            for (int k = 0; k < DFB_LMAX + 2; ++k) {
+                double v = 0.0;
+                if (k <= n) {
+                    v = 1.0;
+                    for (int i = 1; i <= k; ++i) v = v * (double)(n - k + i) / (double)i;
+                }
+                h[n][k] = v;
+            }
+        cudaError_t e = cudaMemcpyToSymbol(c_binom, h, sizeof(h));
+        if (e != cudaSuccess) return set_cuda_error("binomial table upload", e);
+        g_binom_ready[dev] = true;
+    }
+    const int kb = (ci.nef + 31) / 32;
+#define DFB_CASE(K)                                                                                              \
+    if (kb <= K)                                                                                                 \
+        return launch_rys<K, DERIV>(ci, ps, ax, task_pair, task_aux, ntask, naux_grid, mode, out, sP, sM, sN, bar, sbP, sbM, \
+                                    sbN, grad, natm, scratch, scratch_doubles, st, query_only, need);
+    DFB_CASE(1)
+    DFB_CASE(2)
+    DFB_CASE(4)
+    DFB_CASE(8)
+    DFB_CASE(16)
+#undef DFB_CASE
+    return launch_rys<16, DERIV>(ci, ps, ax, task_pair, task_aux, ntask, naux_grid, mode, out, sP, sM, sN, bar, sbP, sbM, sbN,
+                                 grad, natm, scratch, scratch_doubles, st, query_only, need);
+}
+
+}  // namespace dfb
+
+using namespace dfb;
+
+extern "C" int dfb_rys_table_init(const double* coef, const int* offs, long ncoef, const double* herm,
+                                  const int* hoffs, long nherm, int nmax, int nint, int deg, double tmax) {
+    clear_error();
+    if (nmax < 1 || nmax > DFB_NROOTS_MAX || nint < 1 || deg < 0 || !coef || !herm || !offs || !hoffs)
+        return set_error(DFB_ERR_INVALID, "invalid Rys table description");
+    const int dev = current_device();
+    DeviceTable& t = g_tables[dev];
+    if (t.ready) return DFB_OK;
+    cudaError_t e = cudaMalloc(&t.coef, sizeof(double) * ncoef);
+    if (e == cudaSuccess) e = cudaMalloc(&t.herm, sizeof(double) * nherm);
+    if (e == cudaSuccess) e = cudaMemcpy(t.coef, coef, sizeof(double) * ncoef, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(t.herm, herm, sizeof(double) * nherm, cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return set_cuda_error("Rys table upload", e);
+    t.tab.coef = t.coef;
+    t.tab.herm = t.herm;
+    for (int n = 0; n <= DFB_NROOTS_MAX; ++n) {
+        t.tab.offs[n] = (n >= 1 && n <= nmax) ? offs[n] : 0;
+        t.tab.hoff[n] = (n >= 1 && n <= nmax) ? hoffs[n] : 0;
+    }
+    t.tab.nmax = nmax;
+    t.tab.nint = nint;
+    t.tab.deg = deg;
+    t.tab.tmax = tmax;
+    t.ready = true;
+    return DFB_OK;
+}
+
+extern "C" int dfb_pair_tables(const double* cxyz, const int* shell_pstart, const int* shell_nprim,
+                               const double* pexp, const double* pcoef, const int* sp_A, const int* sp_B,
+                               const int* sp_pstart, const int* pp_sp, long npp, int b_dummy, double* eta, double* Px,
+                               double* Py, double* Pz, double* cK, double* ea, double* eb, void* stream) {
+    clear_error();
+    if (npp < 0) return set_error(DFB_ERR_INVALID, "npp < 0");
+    if (npp == 0) return DFB_OK;
+    const unsigned blocks = (unsigned)((npp + 255) / 256);
+    k_pair_tables<<<blocks, 256, 0, (cudaStream_t)stream>>>(cxyz, shell_pstart, shell_nprim, pexp, pcoef, sp_A, sp_B,
+                                                            sp_pstart, pp_sp, npp, b_dummy, eta, Px, Py, Pz, cK, ea,
+                                                            eb);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return set_cuda_error("k_pair_tables launch", e);
+    return DFB_OK;
+}
+
+extern "C" int dfb_rys_int(int la, int lb, int lc, const dfb_pair_side_t* ps, const dfb_aux_side_t* aux,
+                           const int* task_pair, const int* task_aux, long ntask, long naux_grid, int mode, double* out, long sP,
+                           long sM, long sN, double* scratch, long scratch_doubles, void* stream) {
+    clear_error();
+    if (!ps || !aux || (ntask > 0 && (!task_pair || !task_aux || !out)) || (mode != 0 && mode != 1))
+        return set_error(DFB_ERR_INVALID, "invalid arguments to dfb_rys_int");
+    return dispatch_rys<false>(la, lb, lc, ps, aux, task_pair, task_aux, ntask, naux_grid, mode, out, sP, sM, sN, nullptr, 0, 0,
+                               0, nullptr, 0, scratch, scratch_doubles, (cudaStream_t)stream, 0, nullptr);
+}
+
+extern "C" int dfb_rys_deriv(int la, int lb, int lc, const dfb_pair_side_t* ps, const dfb_aux_side_t* aux,
+                             const int* task_pair, const int* task_aux, long ntask, long naux_grid, int mode,
+                             const double* bar,
+                             long sbP, long sbM, long sbN, double* grad, int natm, double* scratch,
+                             long scratch_doubles, void* stream) {
+    clear_error();
+    if (!ps || !aux || (ntask > 0 && (!task_pair || !task_aux || !bar || !grad)) || (mode != 0 && mode != 1) ||
+        natm < 1)
+        return set_error(DFB_ERR_INVALID, "invalid arguments to dfb_rys_deriv");
+    return dispatch_rys<true>(la, lb, lc, ps, aux, task_pair, task_aux, ntask, naux_grid, mode, nullptr, 0, 0, 0, bar, sbP, sbM,
+                              sbN, grad, natm, scratch, scratch_doubles, (cudaStream_t)stream, 0, nullptr);
+}
+
+extern "C" long dfb_rys_scratch_doubles(int la, int lb, int lc, long ntask, int deriv) {
+    clear_error();
+    long need = -1;
+    dfb_pair_side_t ps;
+    dfb_aux_side_t ax;
+    memset(&ps, 0, sizeof(ps));
+    memset(&ax, 0, sizeof(ax));
+    int rc;
+    if (deriv)
+        rc = dispatch_rys<true>(la, lb, lc, &ps, &ax, nullptr, nullptr, ntask, 0, 0, nullptr, 0, 0, 0, nullptr, 0, 0, 0,
+                                nullptr, 1, nullptr, 0, 0, 1, &need);
+    else
+        rc = dispatch_rys<false>(la, lb, lc, &ps, &ax, nullptr, nullptr, ntask, 0, 0, nullptr, 0, 0, 0, nullptr, 0, 0,
+                                 0, nullptr, 1, nullptr, 0, 0, 1, &need);
+    return rc == DFB_OK ? need : (long)rc;
+}

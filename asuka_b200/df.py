@@ -1,0 +1,409 @@
+"""DF integral engine: device-resident bases, pair tables and class task lists.
+
+``DFEngine`` owns everything the Rys kernels of ``libdfb.so`` read for one
+(AO basis, aux basis) pair and exposes
+
+* ``metric()``      -> V[P,Q] = (P|Q)                     (naux, naux)
+* ``int3c(layout)`` -> X = (mu nu|P) as 'Qmn' (naux,nao,nao) or 'mnQ' (nao,nao,naux)
+* ``deriv3c(bar)``  -> sum bar . d(mu nu|P)/dR  accumulated into grad (natm, 3)
+* ``deriv2c(bar)``  -> sum bar . d(P|Q)/dR      accumulated into grad (natm, 3)
+
+and the reference's DF-build seams as module functions with the same names and
+argument meaning (``asuka/cueri/df.py:803,859,946,994``,
+``asuka/integrals/cueri_df.py:33-133``): ``metric_2c2e_basis``,
+``int3c2e_basis``, ``cholesky_metric``, ``whiten_3c2e``,
+``build_df_B_from_cueri_packed_bases``.
+
+Task enumeration follows the reference's unscreened DF build (every l-ordered
+AO shell pair times every aux shell, ``asuka/cueri/gpu.py:1833-1834``; metric
+over unordered aux pairs oriented l(P) >= l(Q), ``gpu.py:1590-1706``); the
+tasks of one angular class go to the device as a (pairs x aux shells) grid.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import functools
+import os
+import weakref
+
+import numpy as np
+import torch
+
+from . import _lib
+from .basis import BasisCartSoA, build_shell_pairs_l_order, from_reference_like, ncart
+
+_DATA = os.path.join(os.path.dirname(os.path.abspath(__file__)), "data")
+_TABLE_READY: set[int] = set()
+NROOTS_SLOTS = 11  # DFB_NROOTS_MAX + 1
+
+
+@functools.lru_cache(maxsize=1)
+def _rys_table_host():
+    with np.load(os.path.join(_DATA, "rys_table.npz")) as z:
+        nmax, tmax, nint, deg = z["meta"]
+        nmax, nint, deg = int(nmax), int(nint), int(deg)
+        coefs, herms = [], []
+        offs = np.zeros(NROOTS_SLOTS, dtype=np.int32)
+        hoffs = np.zeros(NROOTS_SLOTS, dtype=np.int32)
+        o = h = 0
+        for n in range(1, nmax + 1):
+            c = np.ascontiguousarray(z[f"coef{n}"], dtype=np.float64).ravel()
+            w = np.ascontiguousarray(z[f"herm{n}"], dtype=np.float64).ravel()
+            offs[n], hoffs[n] = o, h
+            coefs.append(c)
+            herms.append(w)
+            o += c.size
+            h += w.size
+    return np.concatenate(coefs), offs, np.concatenate(herms), hoffs, nmax, nint, deg, float(tmax)
+
+
+def ensure_rys_table(device: torch.device) -> None:
+    """Upload the Rys node/weight table to ``device`` once per process."""
+    idx = torch.device(device).index
+    idx = torch.cuda.current_device() if idx is None else idx
+    if idx in _TABLE_READY:
+        return
+    coef, offs, herm, hoffs, nmax, nint, deg, tmax = _rys_table_host()
+    L = _lib.lib()
+    with torch.cuda.device(idx):
+        rc = L.dfb_rys_table_init(coef.ctypes.data, offs.ctypes.data, coef.size, herm.ctypes.data, hoffs.ctypes.data,
+                                  herm.size, nmax, nint, deg, tmax)
+    _lib.check(rc, "dfb_rys_table_init")
+    _TABLE_READY.add(idx)
+
+
+def _stream() -> int:
+    return int(torch.cuda.current_stream().cuda_stream)
+
+
+def _as_soa(b) -> BasisCartSoA:
+    return b if isinstance(b, BasisCartSoA) else from_reference_like(b)
+
+
+class DFEngine:
+    """Device-side state of the DF Rys integrals for one (AO, aux) basis pair."""
+
+    def __init__(self, ao_basis, aux_basis, device=None, atom_coords_bohr: np.ndarray | None = None):
+        self.device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
+        if self.device.type != "cuda":
+            raise RuntimeError("DFEngine runs on CUDA devices only (no CPU fallback)")
+        ensure_rys_table(self.device)
+        ao = _as_soa(ao_basis)
+        aux = _as_soa(aux_basis)
+        if ao.shell_atom is None or aux.shell_atom is None:
+            if atom_coords_bohr is None:
+                raise ValueError("bases without shell->atom maps need atom_coords_bohr")
+            from .basis import shell_to_atom_map
+
+            ao = from_reference_like(ao, shell_to_atom_map(ao, atom_coords_bohr))
+            aux = from_reference_like(aux, shell_to_atom_map(aux, atom_coords_bohr))
+        self.ao, self.aux = ao, aux
+        self.nao, self.naux = ao.nao, aux.nao
+        self.natm = int(max(ao.shell_atom.max(initial=-1), aux.shell_atom.max(initial=-1))) + 1
+        if ao.lmax > 8 or aux.lmax > 8:
+            raise NotImplementedError("shells with l > 8 are not supported")
+        dev = self.device
+        i32 = lambda a: torch.as_tensor(np.ascontiguousarray(a, dtype=np.int32), device=dev)  # noqa: E731
+        f64 = lambda a: torch.as_tensor(np.ascontiguousarray(a, dtype=np.float64), device=dev)  # noqa: E731
+
+        # ---- AO side: basis arrays, l-ordered shell pairs, primitive-pair tables
+        self.sp = build_shell_pairs_l_order(ao)
+        self.ao_cxyz = f64(ao.shell_cxyz)
+        self.ao_pstart = i32(ao.shell_prim_start)
+        self.ao_nprim = i32(ao.shell_nprim)
+        self.ao_exp = f64(ao.prim_exp)
+        self.ao_coef = f64(ao.prim_coef)
+        self.ao_aostart = i32(ao.shell_ao_start)
+        self.ao_atom = i32(ao.shell_atom)
+        self.sp_A = i32(self.sp.sp_A)
+        self.sp_B = i32(self.sp.sp_B)
+        self.sp_pstart = i32(self.sp.sp_pair_start[:-1])
+        self.sp_npair = i32(self.sp.sp_npair)
+        self.pp_sp = i32(np.repeat(np.arange(self.sp.nsp, dtype=np.int32), self.sp.sp_npair))
+        npp = int(self.sp.sp_pair_start[-1])
+        self.pt = torch.empty((7, max(npp, 1)), dtype=torch.float64, device=dev)
+
+        # ---- aux side: basis arrays and (P, dummy) self-pair tables for the metric
+        self.ax_cxyz = f64(aux.shell_cxyz)
+        self.ax_pstart = i32(aux.shell_prim_start)
+        self.ax_nprim = i32(aux.shell_nprim)
+        self.ax_exp = f64(aux.prim_exp)
+        self.ax_coef = f64(aux.prim_coef)
+        self.ax_aostart = i32(aux.shell_ao_start)
+        self.ax_atom = i32(aux.shell_atom)
+        self.ax_self = i32(np.arange(aux.nshell, dtype=np.int32))
+        self.ax_pp_sp = i32(np.repeat(np.arange(aux.nshell, dtype=np.int32), aux.shell_nprim))
+        self.axpt = torch.empty((7, max(int(aux.shell_nprim.sum()), 1)), dtype=torch.float64, device=dev)
+        self._build_pair_tables()
+
+        self.ps_ao = _lib.PairSide(
+            *[_lib.ptr(t) for t in (self.sp_A, self.sp_B, self.sp_pstart, self.sp_npair, *self.pt, self.ao_cxyz,
+                                    self.ao_aostart, self.ao_atom)], 0)
+        self.ps_aux = _lib.PairSide(
+            *[_lib.ptr(t) for t in (self.ax_self, self.ax_self, self.ax_pstart, self.ax_nprim, *self.axpt,
+                                    self.ax_cxyz, self.ax_aostart, self.ax_atom)], 1)
+        self.axs = _lib.AuxSide(*[_lib.ptr(t) for t in (self.ax_cxyz, self.ax_pstart, self.ax_nprim, self.ax_exp,
+                                                        self.ax_coef, self.ax_aostart, self.ax_atom)])
+
+        # ---- task classes
+        la = ao.shell_l[self.sp.sp_A]
+        lb = ao.shell_l[self.sp.sp_B]
+        aux_l = aux.shell_l
+        self.aux_by_l = {}
+        for l in np.unique(aux_l):
+            idx = np.nonzero(aux_l == l)[0]
+            idx = idx[np.argsort(aux.shell_nprim[idx], kind="stable")]
+            self.aux_by_l[int(l)] = i32(idx)
+        self.classes3c = []  # (la, lb, lc, pairs tensor, aux tensor)
+        for a in np.unique(la):
+            for b in np.unique(lb):
+                sel = np.nonzero((la == a) & (lb == b))[0]
+                if sel.size == 0:
+                    continue
+                pairs = i32(sel)
+                for c, auxs in self.aux_by_l.items():
+                    self.classes3c.append((int(a), int(b), int(c), pairs, auxs))
+        self.classes2c = []  # (lp, lq, P tensor, Q tensor) explicit lists, P "pair" side
+        nsh = aux.nshell
+        Pi, Qi = np.tril_indices(nsh)
+        lp, lq = aux_l[Pi], aux_l[Qi]
+        swap = lp < lq
+        P = np.where(swap, Qi, Pi)
+        Q = np.where(swap, Pi, Qi)
+        lP, lQ = aux_l[P], aux_l[Q]
+        for a in np.unique(lP):
+            for c in np.unique(lQ):
+                sel = np.nonzero((lP == a) & (lQ == c))[0]
+                if sel.size:
+                    self.classes2c.append((int(a), int(c), i32(P[sel]), i32(Q[sel])))
+        self._scratch = None
+
+    # ------------------------------------------------------------ helpers
+    def _build_pair_tables(self) -> None:
+        L = _lib.lib()
+        p = _lib.ptr
+        npp = int(self.pp_sp.numel())
+        rc = L.dfb_pair_tables(p(self.ao_cxyz), p(self.ao_pstart), p(self.ao_nprim), p(self.ao_exp), p(self.ao_coef),
+                               p(self.sp_A), p(self.sp_B), p(self.sp_pstart), p(self.pp_sp), npp, 0,
+                               *[p(r) for r in self.pt], _stream())
+        _lib.check(rc, "dfb_pair_tables(ao)")
+        nax = int(self.ax_pp_sp.numel())
+        rc = L.dfb_pair_tables(p(self.ax_cxyz), p(self.ax_pstart), p(self.ax_nprim), p(self.ax_exp), p(self.ax_coef),
+                               p(self.ax_self), p(self.ax_self), p(self.ax_pstart), p(self.ax_pp_sp), nax, 1,
+                               *[p(r) for r in self.axpt], _stream())
+        _lib.check(rc, "dfb_pair_tables(aux)")
+
+    def set_coords(self, coords: torch.Tensor) -> None:
+        """Move the shell centres to new atom positions (device tensor (natm, 3), bohr)."""
+        coords = coords.to(device=self.device, dtype=torch.float64).reshape(-1, 3)
+        self.ao_cxyz.copy_(coords.index_select(0, self.ao_atom.long()))
+        self.ax_cxyz.copy_(coords.index_select(0, self.ax_atom.long()))
+        self._build_pair_tables()
+
+    def _scratch_for(self, deriv: bool) -> torch.Tensor:
+        L = _lib.lib()
+        need = 1
+        for la, lb, lc, pairs, auxs in self.classes3c:
+            n = L.dfb_rys_scratch_doubles(la, lb, lc, pairs.numel() * auxs.numel(), int(deriv))
+            _lib.check(0 if n >= 0 else int(n), "dfb_rys_scratch_doubles")
+            need = max(need, n)
+        for lp, lq, P, Q in self.classes2c:
+            n = L.dfb_rys_scratch_doubles(lp, 0, lq, P.numel(), int(deriv))
+            _lib.check(0 if n >= 0 else int(n), "dfb_rys_scratch_doubles")
+            need = max(need, n)
+        if self._scratch is None or self._scratch.numel() < need:
+            self._scratch = torch.empty(need, dtype=torch.float64, device=self.device)
+        return self._scratch
+
+    # ------------------------------------------------------------ integrals
+    def metric(self, out: torch.Tensor | None = None) -> torch.Tensor:
+        """V[P, Q] = (P|Q), full symmetric (naux, naux)."""
+        naux = self.naux
+        V = out if out is not None else torch.empty((naux, naux), dtype=torch.float64, device=self.device)
+        scr = self._scratch_for(False)
+        L = _lib.lib()
+        for lp, lq, P, Q in self.classes2c:
+            rc = L.dfb_rys_int(lp, 0, lq, ctypes.byref(self.ps_aux), ctypes.byref(self.axs), _lib.ptr(P), _lib.ptr(Q),
+                               P.numel(), 0, 1, _lib.ptr(V), naux, 1, 0, _lib.ptr(scr), scr.numel(), _stream())
+            _lib.check(rc, f"dfb_rys_int metric ({lp},{lq})")
+        # diagonal shell blocks are written from one tile in both orders; make V
+        # exactly symmetric as the reference does (cueri_df_cpu.py: V = (V+V^T)/2)
+        V.copy_(0.5 * (V + V.T))
+        return V
+
+    def int3c(self, layout: str = "Qmn", out: torch.Tensor | None = None) -> torch.Tensor:
+        """X = (mu nu|P): 'Qmn' -> (naux, nao, nao), 'mnQ' -> (nao, nao, naux)."""
+        nao, naux = self.nao, self.naux
+        if layout == "Qmn":
+            shape, s = (naux, nao, nao), (nao * nao, nao, 1)
+        elif layout == "mnQ":
+            shape, s = (nao, nao, naux), (1, nao * naux, naux)
+        else:
+            raise ValueError("layout must be 'Qmn' or 'mnQ'")
+        X = out if out is not None else torch.empty(shape, dtype=torch.float64, device=self.device)
+        scr = self._scratch_for(False)
+        L = _lib.lib()
+        for la, lb, lc, pairs, auxs in self.classes3c:
+            rc = L.dfb_rys_int(la, lb, lc, ctypes.byref(self.ps_ao), ctypes.byref(self.axs), _lib.ptr(pairs),
+                               _lib.ptr(auxs), pairs.numel() * auxs.numel(), auxs.numel(), 0, _lib.ptr(X), *s,
+                               _lib.ptr(scr), scr.numel(), _stream())
+            _lib.check(rc, f"dfb_rys_int 3c ({la},{lb},{lc})")
+        return X
+
+    def deriv3c(self, bar: torch.Tensor, grad: torch.Tensor, layout: str = "Qmn") -> torch.Tensor:
+        """grad += sum_{mu nu P} bar[mu nu P] d(mu nu|P)/dR; bar symmetric in (mu, nu)."""
+        nao, naux = self.nao, self.naux
+        if layout == "Qmn":
+            s = (nao * nao, nao, 1)
+        elif layout == "mnQ":
+            s = (1, nao * naux, naux)
+        else:
+            raise ValueError("layout must be 'Qmn' or 'mnQ'")
+        bar = bar.contiguous()
+        scr = self._scratch_for(True)
+        L = _lib.lib()
+        for la, lb, lc, pairs, auxs in self.classes3c:
+            rc = L.dfb_rys_deriv(la, lb, lc, ctypes.byref(self.ps_ao), ctypes.byref(self.axs), _lib.ptr(pairs),
+                                 _lib.ptr(auxs), pairs.numel() * auxs.numel(), auxs.numel(), 0, _lib.ptr(bar), *s,
+                                 _lib.ptr(grad), self.natm, _lib.ptr(scr), scr.numel(), _stream())
+            _lib.check(rc, f"dfb_rys_deriv 3c ({la},{lb},{lc})")
+        return grad
+
+    def deriv2c(self, bar: torch.Tensor, grad: torch.Tensor) -> torch.Tensor:
+        """grad += sum_{P,Q} bar[P,Q] d(P|Q)/dR; bar symmetric."""
+        naux = self.naux
+        bar = bar.contiguous()
+        scr = self._scratch_for(True)
+        L = _lib.lib()
+        for lp, lq, P, Q in self.classes2c:
+            rc = L.dfb_rys_deriv(lp, 0, lq, ctypes.byref(self.ps_aux), ctypes.byref(self.axs), _lib.ptr(P),
+                                 _lib.ptr(Q), P.numel(), 0, 1, _lib.ptr(bar), naux, 1, 0, _lib.ptr(grad), self.natm,
+                                 _lib.ptr(scr), scr.numel(), _stream())
+            _lib.check(rc, f"dfb_rys_deriv metric ({lp},{lq})")
+        return grad
+
+
+# ---------------------------------------------------------------- reference seams
+
+_ENGINES: "weakref.WeakValueDictionary" = weakref.WeakValueDictionary()
+_ENGINE_KEEP: dict = {}
+
+
+def get_engine(ao_basis, aux_basis, device=None) -> DFEngine:
+    """Engine cached by (id(ao), id(aux), device) like the reference's plan caches (gpu.py:1602-1612)."""
+    dev = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
+    key = (id(ao_basis), id(aux_basis), dev.index)
+    eng = _ENGINE_KEEP.get(key)
+    if eng is None or eng._bases_ref[0]() is not ao_basis or eng._bases_ref[1]() is not aux_basis:
+        eng = DFEngine(ao_basis, aux_basis, device=dev)
+        try:
+            eng._bases_ref = (weakref.ref(ao_basis), weakref.ref(aux_basis))
+        except TypeError:
+            eng._bases_ref = (lambda: ao_basis, lambda: aux_basis)
+        if len(_ENGINE_KEEP) > 8:
+            _ENGINE_KEEP.clear()
+        _ENGINE_KEEP[key] = eng
+    return eng
+
+
+def _dummy_ao_for(aux_basis):
+    """Metric-only engines still need an AO side; an s shell at the first aux centre works."""
+    aux = _as_soa(aux_basis)
+    return BasisCartSoA(shell_cxyz=aux.shell_cxyz[:1].copy(), shell_prim_start=np.zeros(1, np.int32),
+                        shell_nprim=np.ones(1, np.int32), shell_l=np.zeros(1, np.int32),
+                        shell_ao_start=np.zeros(1, np.int32), prim_exp=np.ones(1), prim_coef=np.ones(1),
+                        shell_atom=None if aux.shell_atom is None else aux.shell_atom[:1].copy())
+
+
+def metric_2c2e_basis(aux_basis, *, stream=None, backend: str = "gpu_rys", mode: str = "warp", threads: int = 256,
+                      mixed_precision: bool = False, atom_coords_bohr=None) -> torch.Tensor:
+    """V[P,Q] = (P|Q) on the current CUDA device (``asuka/cueri/df.py:803``)."""
+    if backend not in ("gpu_rys", "gpu_sp", "gpu_ss"):
+        raise ValueError("backend must be one of gpu_rys/gpu_sp/gpu_ss")
+    aux = _as_soa(aux_basis)
+    if aux.shell_atom is None:
+        aux = from_reference_like(aux, np.zeros(aux.nshell, np.int32))
+    eng = DFEngine(_dummy_ao_for(aux), aux)
+    return eng.metric()
+
+
+def int3c2e_basis(ao_basis, aux_basis, *, stream=None, backend: str = "gpu_rys", mode: str = "warp",
+                  threads: int = 256, mixed_precision: bool = False, layout: str = "mnQ") -> torch.Tensor:
+    """X[mu,nu,P] = (mu nu|P) (``asuka/cueri/df.py:859``); layout 'mnQ' or 'Qmn'."""
+    ao, aux = _as_soa(ao_basis), _as_soa(aux_basis)
+    if ao.shell_atom is None:
+        ao = from_reference_like(ao, np.zeros(ao.nshell, np.int32))
+    if aux.shell_atom is None:
+        aux = from_reference_like(aux, np.zeros(aux.nshell, np.int32))
+    return DFEngine(ao, aux).int3c(layout)
+
+
+def cholesky_metric(V: torch.Tensor, *, shift: float = 0.0) -> torch.Tensor:
+    """Lower Cholesky factor of the metric.
+
+    The reference's CPU DF build factorises V with no diagonal shift
+    (``asuka/integrals/cueri_df_cpu.py:521``); that is the default here, so FP64
+    results match the reference CPU path.  A non-zero ``shift`` is added to the
+    diagonal first, as the reference's GPU builder does (``cueri_df.py:86-89``).
+    """
+    Vs = 0.5 * (V + V.T)
+    if shift:
+        Vs = Vs + float(shift) * torch.eye(V.shape[0], dtype=V.dtype, device=V.device)
+    L, info = torch.linalg.cholesky_ex(Vs)
+    if int(info.item()) != 0:
+        raise RuntimeError(f"metric Cholesky failed (leading minor {int(info.item())} not positive definite)")
+    return L
+
+
+def whiten_3c2e(X: torch.Tensor, L: torch.Tensor, layout: str = "mnQ") -> torch.Tensor:
+    """B = X L^-T over the aux index, in place (``asuka/cueri/df.py:994``)."""
+    if layout == "mnQ":
+        nao = X.shape[0]
+        X2 = X.view(nao * nao, -1)
+        # B^T = L^-1 X^T  <=>  B = X L^-T
+        X2.copy_(torch.linalg.solve_triangular(L, X2.T, upper=False).T)
+        return X
+    if layout == "Qmn":
+        naux = X.shape[0]
+        X2 = X.view(naux, -1)
+        X2.copy_(torch.linalg.solve_triangular(L, X2, upper=False))
+        return X
+    raise ValueError("layout must be 'mnQ' or 'Qmn'")
+
+
+def build_df_B_from_cueri_packed_bases(ao_basis, aux_basis, *, config=None, layout: str = "mnQ",
+                                       ao_rep: str = "cart", profile: dict | None = None, return_L: bool = False):
+    """Whitened DF factors B with (mu nu|ls) ~= sum_Q B[mu nu Q] B[ls Q] (``asuka/integrals/cueri_df.py:33``).
+
+    FP64 device tensors; ``layout='mnQ'`` -> (nao, nao, naux), ``'Qmn'`` -> (naux, nao, nao).
+    Errors raise RuntimeError/ValueError/NotImplementedError; there is no CPU fallback.
+    """
+    if ao_rep != "cart":
+        raise NotImplementedError("ao_rep='sph' is not implemented (Cartesian AOs only)")
+    ao, aux = _as_soa(ao_basis), _as_soa(aux_basis)
+    if ao.shell_atom is None:
+        ao = from_reference_like(ao, np.zeros(ao.nshell, np.int32))
+    if aux.shell_atom is None:
+        aux = from_reference_like(aux, np.zeros(aux.nshell, np.int32))
+    eng = DFEngine(ao, aux)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(5)] if profile is not None else None
+    if ev:
+        ev[0].record()
+    V = eng.metric()
+    if ev:
+        ev[1].record()
+    X = eng.int3c(layout)
+    if ev:
+        ev[2].record()
+    L = cholesky_metric(V)
+    if ev:
+        ev[3].record()
+    B = whiten_3c2e(X, L, layout)
+    if ev:
+        ev[4].record()
+        torch.cuda.synchronize()
+        profile.update(t_metric_s=ev[0].elapsed_time(ev[1]) / 1e3, t_int3c2e_s=ev[1].elapsed_time(ev[2]) / 1e3,
+                       t_metric_cholesky_s=ev[2].elapsed_time(ev[3]) / 1e3,
+                       t_whiten_s=ev[3].elapsed_time(ev[4]) / 1e3, nao=eng.nao, naux=eng.naux)
+    return (B, L) if return_L else B
