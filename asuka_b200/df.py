@@ -216,6 +216,54 @@ class DFEngine:
             self._scratch = torch.empty(need, dtype=torch.float64, device=self.device)
         return self._scratch
 
+    def aux_blocks(self, max_naux: int = 256):
+        """Contiguous aux-shell blocks of at most ``max_naux`` functions, aligned to shells
+        (``asuka/cueri/df.py:2059-2119`` plan_aux_blocks_cart); returns (p0, p1, AuxSide) tuples."""
+        if getattr(self, "_aux_blocks_n", None) == max_naux:
+            return self._aux_blocks
+        aux = self.aux
+        nc = np.array([ncart(int(l)) for l in aux.shell_l])
+        blocks = []
+        s0 = 0
+        while s0 < aux.nshell:
+            s1 = s0
+            tot = 0
+            while s1 < aux.nshell and (tot + nc[s1] <= max_naux or s1 == s0):
+                tot += nc[s1]
+                s1 += 1
+            p0 = int(aux.shell_ao_start[s0])
+            p1 = p0 + int(tot)
+            shifted = torch.as_tensor(aux.shell_ao_start.astype(np.int32) - p0, device=self.device)
+            axb = _lib.AuxSide(*[_lib.ptr(t) for t in (self.ax_cxyz, self.ax_pstart, self.ax_nprim, self.ax_exp,
+                                                       self.ax_coef, shifted, self.ax_atom)])
+            byl = {}
+            for l in np.unique(aux.shell_l[s0:s1]):
+                idx = s0 + np.nonzero(aux.shell_l[s0:s1] == l)[0]
+                byl[int(l)] = torch.as_tensor(idx.astype(np.int32), device=self.device)
+            blocks.append((p0, p1, (axb, shifted, byl)))
+            s0 = s1
+        self._aux_blocks, self._aux_blocks_n = blocks, max_naux
+        return blocks
+
+    def int3c_block(self, blk, p0: int, p1: int, out: torch.Tensor | None = None) -> torch.Tensor:
+        """X rows for one aux block as (p1-p0, nao, nao) (streamed DF, ``gpu.py:2742``)."""
+        axb, _shifted, byl = blk
+        nao = self.nao
+        X = out if out is not None else torch.empty((p1 - p0, nao, nao), dtype=torch.float64, device=self.device)
+        scr = self._scratch_for(False)
+        L = _lib.lib()
+        seen = set()
+        for la, lb, lc, pairs, _auxs in self.classes3c:
+            if lc not in byl or (la, lb, lc) in seen:
+                continue
+            seen.add((la, lb, lc))
+            auxs = byl[lc]
+            rc = L.dfb_rys_int(la, lb, lc, ctypes.byref(self.ps_ao), ctypes.byref(axb), _lib.ptr(pairs),
+                               _lib.ptr(auxs), pairs.numel() * auxs.numel(), auxs.numel(), 0, _lib.ptr(X),
+                               nao * nao, nao, 1, _lib.ptr(scr), scr.numel(), _stream())
+            _lib.check(rc, f"dfb_rys_int 3c block ({la},{lb},{lc})")
+        return X
+
     # ------------------------------------------------------------ integrals
     def metric(self, out: torch.Tensor | None = None) -> torch.Tensor:
         """V[P, Q] = (P|Q), full symmetric (naux, naux)."""

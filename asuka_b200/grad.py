@@ -1,0 +1,154 @@
+"""DF two-electron energy and its nuclear gradient.
+
+``DFEnergyFunction`` is a ``torch.autograd.Function`` whose forward maps
+(nuclear coordinates R, weighted occupied orbitals Cw with D = Cw Cw^T) to
+(E_2e, J, K), building the DF integrals at R on the GPU, and whose backward
+returns dE_2e/dR from the Rys derivative integrals contracted on the fly with
+the adjoints (and dE_2e/dCw = 2 (J - K/2) Cw).
+
+Forward, with X_P = (mu nu|P), V = L L^T:
+    rho = X . D,  d = V^-1 rho,  J = sum_P d_P X_P
+    Y_P = X_P Cw, W = L^-1 Y,    K = sum_Q W_Q W_Q^T
+    E_2e = 1/2 rho.d - 1/4 tr(D K)
+Backward (M_Q = Cw^T W_Q, Z = L^-T M):
+    dE/dX_P = d_P D - 1/2 Cw Z_P Cw^T
+    dE/dV   = -1/2 d d^T + 1/4 Z Z^T          (Z as naux x nocc^2)
+    dE/dR   = sum dE/dX . dX/dR + sum dE/dV . dV/dR
+This equals the reference's whitened-factor route (bar_L = rho_Q D - 1/2 D B_Q D
+through ``df_whiten_adjoint_Qmn``/``chol_lower_adjoint``,
+``asuka/integrals/df_adjoint.py:172-235,322-361``) without the two
+naux^2 nao^2 triangular solves.
+
+``compute_df_gradient_contributions_analytic_packed_bases`` keeps the
+reference's signature and whitened-factor adjoints
+(``asuka/integrals/grad.py:114-723``) for callers that hold B and dE/dB.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+import torch
+
+from . import mixed as _mixed
+from .df import DFEngine, cholesky_metric
+
+
+def _mm(A, B, precision):
+    return A @ B if precision == "fp64" else _mixed.matmul(A, B)
+
+
+def df_forward(engine: DFEngine, Cw: torch.Tensor, precision: str = "fp64", X: torch.Tensor | None = None):
+    """Integrals at the engine's current geometry, then (E_2e, J, K) and the saved intermediates."""
+    nao, naux = engine.nao, engine.naux
+    nocc = Cw.shape[1]
+    V = engine.metric()
+    L = cholesky_metric(V)
+    X = engine.int3c("Qmn", out=X)
+    X2 = X.view(naux, nao * nao)
+    D = Cw @ Cw.T
+    D = 0.5 * (D + D.T)
+    rho = X2 @ D.reshape(-1)
+    d = torch.cholesky_solve(rho.view(-1, 1), L).view(-1)
+    J = (d @ X2).view(nao, nao)
+    J = 0.5 * (J + J.T)
+    Y = _mm(X.view(naux * nao, nao), Cw, precision).view(naux, nao * nocc)
+    W = torch.linalg.solve_triangular(L, Y, upper=False)
+    W2 = W.view(naux, nao, nocc).permute(1, 0, 2).reshape(nao, naux * nocc)
+    K = _mm(W2, W2.T.contiguous(), precision) if precision != "fp64" else W2 @ W2.T
+    K = 0.5 * (K + K.T)
+    E = 0.5 * torch.dot(rho, d) - 0.25 * torch.sum(D * K)
+    return E, J, K, dict(X=X, L=L, d=d, W=W, D=D)
+
+
+def df_backward(engine: DFEngine, Cw: torch.Tensor, saved: dict, grad: torch.Tensor | None = None,
+                precision: str = "fp64") -> torch.Tensor:
+    """dE_2e/dR accumulated into grad (natm, 3)."""
+    nao, naux = engine.nao, engine.naux
+    nocc = Cw.shape[1]
+    X, L, d, W, D = saved["X"], saved["L"], saved["d"], saved["W"], saved["D"]
+    # M_Q = Cw^T W_Q  (naux, nocc, nocc)
+    M = torch.matmul(Cw.T, W.view(naux, nao, nocc))
+    M = 0.5 * (M + M.transpose(1, 2))
+    Z = torch.linalg.solve_triangular(L.T, M.reshape(naux, nocc * nocc), upper=True)
+    Zq = Z.view(naux, nocc, nocc)
+    # Gamma_P = d_P D - 1/2 Cw Z_P Cw^T, written over X's storage (X is not needed afterwards)
+    G3 = X
+    T = torch.matmul(Zq, Cw.T)  # (naux, nocc, nao)
+    torch.matmul(Cw, T, out=G3)
+    G3.mul_(-0.5).add_(d.view(naux, 1, 1) * D.view(1, nao, nao))
+    G2 = -0.5 * torch.outer(d, d) + 0.25 * (Z @ Z.T)
+    if grad is None:
+        grad = torch.zeros((engine.natm, 3), dtype=torch.float64, device=X.device)
+    engine.deriv3c(G3, grad, layout="Qmn")
+    engine.deriv2c(G2, grad)
+    return grad
+
+
+class DFEnergyFunction(torch.autograd.Function):
+    """(R, Cw) -> (E_2e, J, K); backward gives dE_2e/dR and dE_2e/dCw."""
+
+    @staticmethod
+    def forward(ctx, coords: torch.Tensor, Cw: torch.Tensor, engine: DFEngine, precision: str = "fp64"):
+        engine.set_coords(coords.detach())
+        E, J, K, saved = df_forward(engine, Cw.detach(), precision)
+        ctx.engine = engine
+        ctx.precision = precision
+        ctx.saved = saved
+        ctx.save_for_backward(Cw.detach(), J, K)
+        ctx.mark_non_differentiable(J, K)
+        return E, J, K
+
+    @staticmethod
+    def backward(ctx, gE, gJ, gK):
+        Cw, J, K = ctx.saved_tensors
+        g = df_backward(ctx.engine, Cw, ctx.saved, precision=ctx.precision)
+        ctx.saved = None
+        gCw = 2.0 * ((J - 0.5 * K) @ Cw)
+        return g * gE, gCw * gE, None, None
+
+
+def df_energy(coords: torch.Tensor, Cw: torch.Tensor, engine: DFEngine, precision: str = "fp64"):
+    """Differentiable E_2e(R, Cw); returns (E, J, K)."""
+    return DFEnergyFunction.apply(coords, Cw, engine, precision)
+
+
+# ---------------------------------------------------------------- reference seam
+
+def compute_df_gradient_contributions_analytic_packed_bases(ao_basis, aux_basis, *, atom_coords_bohr, B_ao,
+                                                            bar_L_ao, L_chol=None, backend: str = "cuda",
+                                                            df_threads: int = 0, profile: dict | None = None):
+    """DF 2e gradient from whitened factors B (nao,nao,naux) and dE/dB (naux,nao,nao); returns (natm, 3).
+
+    Same contract as ``asuka/integrals/grad.py:114``: backprop through the
+    whitening and the metric Cholesky to the unwhitened integrals, then contract
+    the analytic integral derivatives.  Runs on the GPU (``backend`` must be
+    'cuda' or 'gpu'; there is no CPU path).
+    """
+    if str(backend).lower() not in ("cuda", "gpu"):
+        raise ValueError("this engine runs on the GPU only (backend='cuda')")
+    R = np.asarray(atom_coords_bohr, dtype=np.float64).reshape((-1, 3))
+    natm = R.shape[0]
+    eng = DFEngine(ao_basis, aux_basis, atom_coords_bohr=R)
+    dev = eng.device
+    B = torch.as_tensor(B_ao, dtype=torch.float64, device=dev).contiguous()
+    barL = torch.as_tensor(bar_L_ao, dtype=torch.float64, device=dev).contiguous()
+    nao, _, naux = B.shape
+    if barL.shape != (naux, nao, nao):
+        raise ValueError("bar_L_ao must have shape (naux, nao, nao)")
+    if L_chol is not None:
+        L = torch.as_tensor(L_chol, dtype=torch.float64, device=dev)
+    else:
+        L = cholesky_metric(eng.metric())
+    tmp = torch.linalg.solve_triangular(L.T, barL.view(naux, nao * nao), upper=True)  # L^-T bar_B^T
+    bar_Lc = -torch.tril(tmp @ B.view(nao * nao, naux))
+    bar_X = tmp.view(naux, nao, nao)
+    bar_X = 0.5 * (bar_X + bar_X.transpose(1, 2))
+    G = torch.tril(L.T @ bar_Lc)
+    G.diagonal().mul_(0.5)
+    t2 = torch.linalg.solve_triangular(L.T, G, upper=True)
+    bar_V = torch.linalg.solve_triangular(L.T, t2.T, upper=True).T
+    bar_V = 0.5 * (bar_V + bar_V.T)
+    grad = torch.zeros((natm, 3), dtype=torch.float64, device=dev)
+    eng.deriv3c(bar_X.contiguous(), grad, layout="Qmn")
+    eng.deriv2c(bar_V.contiguous(), grad)
+    return grad.cpu().numpy()

@@ -1,0 +1,394 @@
+"""Benchmark: ms per DF J/K build + nuclear gradient on one B200 (mixed vs FP64).
+
+Workload: (H2O)_8 water cluster, seed 0 (O-H 0.9572 A, HOH 104.52 deg, min O-O
+2.7 A), ma-TZVP Cartesian AO basis (stand-in for cc-pVTZ: same maximum l) +
+RICD acCD auxiliary basis: 416 AO / 1824 aux functions.
+
+One step = forward + backward of the DF two-electron energy at the converged
+RHF density: DF integrals at R (pair tables, metric (P|Q), Cholesky, 3c
+(mu nu|P)), J/K and E_2e, then dE_2e/dR (adjoints + derivative Rys integrals
+contracted on the fly).  ``value`` times it with inputs resident on the GPU;
+``e2e`` times the same call through the public API from pinned host buffers
+(coordinates and occupied orbitals in, energy and gradient out).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+With N > 1 (torchrun) every rank runs an independent replica of the step
+(the north-star path is single-GPU; see DESIGN.md "replicas only").
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "ms per DF J/K build + nuclear gradient, mixed vs FP64 on 1 B200 at |dE|<=1e-6 Eh"
+WORKLOAD = "(H2O)8 seed 0, ma-TZVP cart (cc-pVTZ stand-in) + RICD aux, 416 AO / 1824 aux"
+
+
+def _peaks() -> dict:
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        with open(p) as f:
+            return json.load(f)
+    return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "_fallback": True}
+
+
+def _workload():
+    from asuka_b200 import basis as bm
+    from asuka_b200 import geometry as geo
+
+    mol = geo.water_cluster(8, 0, "ma-tzvp")
+    atoms = list(mol.atoms_bohr)
+    return mol, bm.pack_basis(atoms, "ma-tzvp", "ao"), bm.pack_basis(atoms, "ma-tzvp", "aux")
+
+
+def flops_deriv3c(ao, aux) -> float:
+    """Algorithmic FLOPs of the 3c derivative contraction (per-unit model of the survey, 8(d))."""
+    from asuka_b200.basis import build_shell_pairs_l_order, ncart
+
+    sp = build_shell_pairs_l_order(ao)
+    la = ao.shell_l[sp.sp_A]
+    lb = ao.shell_l[sp.sp_B]
+    tot = 0.0
+    for lp in np.unique(aux.shell_l):
+        kp = float(aux.shell_nprim[aux.shell_l == lp].sum())
+        for a in np.unique(la):
+            for b in np.unique(lb):
+                m = (la == a) & (lb == b)
+                if not m.any():
+                    continue
+                kab = float(sp.sp_npair[m].sum())
+                nr = (a + b + lp + 1) // 2 + 1
+                n3 = ncart(int(a)) * ncart(int(b)) * ncart(int(lp))
+                tot += kab * kp * nr * (n3 * 25 + 9 * (a + b + 2) * (lp + 2))
+    return tot
+
+
+class ClockSampler:
+    def __init__(self):
+        self.p = None
+        self.rows = []
+
+    def __enter__(self):
+        try:
+            self.p = subprocess.Popen(
+                ["nvidia-smi", "--query-gpu=index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+                 "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
+                 "--format=csv,noheader,nounits", "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL,
+                text=True)
+        except Exception:
+            self.p = None
+        return self
+
+    def __exit__(self, *a):
+        if self.p is None:
+            return
+        self.p.terminate()
+        try:
+            out, _ = self.p.communicate(timeout=5)
+        except Exception:
+            self.p.kill()
+            out = ""
+        dev = os.environ.get("LOCAL_RANK", "0")
+        for line in out.splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) >= 9 and f[0] == dev:
+                self.rows.append(f)
+
+    def summary(self) -> dict:
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        reasons = set()
+        for r in self.rows:
+            for name, v in zip(("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"), r[5:9]):
+                if v.strip().lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(self.rows)}
+
+
+def _dist_setup(n_gpus: int):
+    import torch
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    elif torch.cuda.is_available():
+        torch.cuda.set_device(0)
+    return rank, world, local
+
+
+def _reduce_max(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def _barrier(world: int) -> None:
+    import torch
+
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+    torch.cuda.synchronize()
+
+
+def run_reference(args) -> dict:
+    """CPU reference arm: the reference's Cython Rys kernels + its DF algebra on the host cores."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import ref_cpu
+
+    mol, ao, aux = _workload()
+    cores = os.cpu_count() or 1
+    os.environ.setdefault("OMP_NUM_THREADS", str(cores))
+    if not ref_cpu.available():
+        return {"impl": "reference", "unavailable": "reference CPU kernels not built (oracle/build_ref.py)"}
+    rng = np.random.default_rng(0)
+    # a density-like occupied block of the right size (cost does not depend on the values)
+    Cw = np.linalg.qr(rng.standard_normal((ao.nao, mol.nelectron // 2)))[0] * np.sqrt(2.0)
+    stride = int(os.environ.get("DFB_REF_PAIR_STRIDE", "400"))
+    times = []
+    for i in range(args.warmup + args.steps):
+        r = ref_cpu.cpu_step(ao, aux, Cw, mol.natm, pair_stride=stride, threads=0)
+        if i >= args.warmup:
+            times.append(r["total"])
+    ms = 1e3 * float(np.mean(times))
+    frac = r["sample_fraction"]
+    return {"metric": METRIC, "value": ms, "unit": "ms", "impl": "reference", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": WORKLOAD, "precision": "fp64 (reference CPU)"},
+            "cpu_baseline": {"value": ms, "unit": "ms", "cores": cores, "kind": "reference",
+                             "sample": f"3c and 3c-derivative loops over every {stride}th AO shell pair "
+                                       f"({100 * frac:.2f}% of primitive-pair work), scaled; metric, Cholesky, "
+                                       f"whitening, J/K, adjoints, 2c derivatives at full size"},
+            "e2e": {"value": ms, "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "phases_s": {k: round(v, 4) for k, v in r.items() if isinstance(v, float) and k != "E2"}}
+
+
+def run_gpu(args) -> dict | None:
+    import torch
+
+    from asuka_b200 import df as dfmod
+    from asuka_b200.df import DFEngine
+    from asuka_b200.grad import df_backward, df_energy, df_forward
+    from asuka_b200.int1e import build_int1e
+    from asuka_b200.scf import rhf_df
+
+    rank, world, local = _dist_setup(args.gpus)
+    dev = torch.device("cuda", local if world > 1 else 0)
+    mol, ao, aux = _workload()
+    eng = DFEngine(ao, aux, device=dev)
+    nao, naux = eng.nao, eng.naux
+    # converged RHF density (outside the timed region), mixed-then-FP64 and all-FP64
+    int1e = build_int1e(ao, mol.coords_bohr, mol.charges, device=dev)
+    from asuka_b200.df import cholesky_metric, whiten_3c2e
+
+    L = cholesky_metric(eng.metric())
+    B = whiten_3c2e(eng.int3c("Qmn"), L, layout="Qmn")
+    scf64 = rhf_df(int1e.S, int1e.hcore, B, nelec=mol.nelectron, enuc=mol.energy_nuc())
+    scfmx = rhf_df(int1e.S, int1e.hcore, B, nelec=mol.nelectron, enuc=mol.energy_nuc(), precision="mixed")
+    del B
+    torch.cuda.empty_cache()
+    nocc = mol.nelectron // 2
+    Cw = (scf64.mo_coeff[:, :nocc] * 2.0**0.5).contiguous()
+    R = torch.as_tensor(mol.coords_bohr, dtype=torch.float64, device=dev)
+    X = torch.empty((naux, nao, nao), dtype=torch.float64, device=dev)
+
+    def step(prec):
+        eng.set_coords(R)
+        E, J, K, saved = df_forward(eng, Cw, prec, X=X)
+        g = df_backward(eng, Cw, saved, precision=prec)
+        return E, g
+
+    # accuracy of the mixed step against the FP64 step (same inputs)
+    E64, g64 = step("fp64")
+    Emx, gmx = step("mixed")
+    dE_step = abs(float(E64) - float(Emx))
+    dG_step = float((g64 - gmx).abs().max())
+
+    # count our kernel launches in one step
+    import asuka_b200._lib as _l
+
+    calls = {"n": 0}
+    real = _l.lib()
+    orig = {n: getattr(real, n) for n in ("dfb_rys_int", "dfb_rys_deriv", "dfb_pair_tables")}
+
+    class _Count:
+        def __getattr__(self, n):
+            f = orig.get(n)
+            if f is None:
+                return getattr(real, n)
+
+            def w(*a):
+                calls["n"] += 1
+                return f(*a)
+
+            return w
+
+    _l._LIB = _Count()
+    step("mixed")
+    _l._LIB = real
+    launches_per_step = calls["n"]
+
+    stream = torch.cuda.current_stream(dev)
+    results = {}
+    for prec in ("fp64", "mixed"):
+        for _ in range(args.warmup):
+            step(prec)
+        _barrier(world)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with ClockSampler() as cs:
+            e0.record(stream)
+            for _ in range(args.steps):
+                step(prec)
+            e1.record(stream)
+            _barrier(world)
+        results[prec] = (_reduce_max(e0.elapsed_time(e1) / args.steps, world), cs.summary())
+
+    # roofline of the dominant kernel family: the 3c derivative contraction (FP64 CUDA cores)
+    E, J, K, saved = df_forward(eng, Cw, "mixed", X=X)
+    G3 = saved["X"]
+    gbuf = torch.zeros((eng.natm, 3), dtype=torch.float64, device=dev)
+    for _ in range(2):
+        eng.deriv3c(G3, gbuf)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    nrep = 3
+    e0.record(stream)
+    for _ in range(nrep):
+        eng.deriv3c(G3, gbuf)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    t_d3 = e0.elapsed_time(e1) / nrep
+    fl = flops_deriv3c(ao, aux)
+    from asuka_b200.peaks import fp64_dgemm_tflops, fp64_fma_tflops
+
+    fp64_peak = fp64_fma_tflops(dev)
+    fp64_src = "measured live: FP64 FMA probe (dfb_fp64_fma_probe), all SMs, best of 5"
+    dgemm_peak = fp64_dgemm_tflops(4096, dev)
+    achieved = fl / (t_d3 * 1e-3) / 1e12
+    del X, saved, G3
+    torch.cuda.empty_cache()
+
+    # end to end through the public API from pinned host buffers
+    Rh = torch.as_tensor(mol.coords_bohr, dtype=torch.float64).pin_memory()
+    Cwh = Cw.cpu().pin_memory()
+    gh = torch.empty((mol.natm, 3), dtype=torch.float64).pin_memory()
+    Eh = torch.empty((), dtype=torch.float64).pin_memory()
+
+    def e2e_step():
+        Rd = Rh.to(dev, non_blocking=True).requires_grad_(True)
+        Cd = Cwh.to(dev, non_blocking=True)
+        Ed, _, _ = df_energy(Rd, Cd, eng, "mixed")
+        (gd,) = torch.autograd.grad(Ed, Rd)
+        gh.copy_(gd, non_blocking=True)
+        Eh.copy_(Ed.detach(), non_blocking=True)
+
+    for _ in range(args.warmup):
+        e2e_step()
+    _barrier(world)
+    e0.record(stream)
+    for _ in range(args.steps):
+        e2e_step()
+    e1.record(stream)
+    _barrier(world)
+    t_e2e = _reduce_max(e0.elapsed_time(e1) / args.steps, world)
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+    if rank != 0:
+        return None
+
+    ms_mx, clk = results["mixed"]
+    ms_64, clk64 = results["fp64"]
+    out = {
+        "metric": METRIC, "value": round(ms_mx, 4), "unit": "ms", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(ms_mx, 4), "higher_is_better": False, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded geometry; basis tables from the reference)",
+        "config": {"workload": WORKLOAD, "nao": nao, "naux": naux, "precision": "mixed (split-BF16 J/K contractions,"
+                   " FP64 integrals and gradient accumulation)", "l2": "working set (3c tensor 2.5 GB) > L2 126 MB",
+                   "replicas": world if world > 1 else None},
+        "fp64_ms_per_step": round(ms_64, 4),
+        "mixed_speedup_vs_fp64": round(ms_64 / ms_mx, 4),
+        "accuracy": {"scf_dE_mixed_vs_fp64_Eh": abs(scfmx.e_tot - scf64.e_tot), "scf_e_tot": scf64.e_tot,
+                     "scf_iters_fp64": scf64.niter, "scf_iters_mixed": scfmx.niter,
+                     "step_dE2_mixed_vs_fp64_Eh": dE_step, "step_max_dgrad_Eh_per_bohr": dG_step},
+        "e2e": {"value": round(t_e2e, 4), "unit": "ms", "h2d_bytes_per_step": int(Rh.numel() * 8 + Cwh.numel() * 8),
+                "d2h_bytes_per_step": int(gh.numel() * 8 + 8)},
+        "gpu_launches": int(launches_per_step * args.steps),
+        "roofline": {"kernel": "k_rys<DERIV> (3c derivative contraction, all classes)", "bound": "fp64",
+                     "achieved": round(achieved, 3), "peak": fp64_peak, "unit": "TFLOP/s",
+                     "frac": round(achieved / fp64_peak, 4), "peak_source": fp64_src,
+                     "fp64_dgemm_tflops": round(dgemm_peak, 2),
+                     "avg_launch_set_ms": round(t_d3, 4), "algorithmic_flops": fl, "traffic": None},
+        "clocks": clk, "clocks_fp64_run": clk64,
+    }
+    if not args.no_cpu_baseline:
+        try:
+            sys.path.insert(0, os.path.join(ROOT, "oracle"))
+            import ref_cpu
+
+            if ref_cpu.available():
+                cores = os.cpu_count() or 1
+                stride = int(os.environ.get("DFB_REF_PAIR_STRIDE", "400"))
+                r = ref_cpu.cpu_step(ao, aux, Cw.cpu().numpy(), mol.natm, pair_stride=stride)
+                out["cpu_baseline"] = {"value": round(1e3 * r["total"], 1), "unit": "ms", "cores": cores,
+                                       "kind": "reference",
+                                       "sample": f"3c loops over every {stride}th AO shell pair "
+                                                 f"({100 * r['sample_fraction']:.2f}% of primitive-pair work), "
+                                                 "scaled; rest at full size"}
+        except Exception as exc:  # the baseline is reported, never required
+            out["cpu_baseline"] = {"value": None, "error": str(exc)[:200]}
+    return out
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        rank = int(os.environ.get("RANK", "0"))
+        if rank != 0:
+            return
+        print(json.dumps(run_reference(args)), flush=True)
+        return
+    out = run_gpu(args)
+    if out is not None:
+        print(json.dumps(out), flush=True)
+
+
+if __name__ == "__main__":
+    main()

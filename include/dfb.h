@@ -107,6 +107,13 @@ int dfb_rys_deriv(int la, int lb, int lc, const dfb_pair_side_t *ps, const dfb_a
                   const int *task_pair, const int *task_aux, long ntask, long naux_grid, int mode, const double *bar, long sbP,
                   long sbM, long sbN, double *grad, int natm, double *scratch, long scratch_doubles, void *stream);
 
+/*
+ * FP64 FMA throughput probe: blocks x threads threads each run iters x 64
+ * dependent-chain FMAs (8 chains); out holds blocks*threads doubles.  Used to
+ * measure the FP64 peak that bounds the Rys kernels (no reference counterpart).
+ */
+int dfb_fp64_fma_probe(double *out, int blocks, int threads, int iters, void *stream);
+
 /* Scratch doubles dfb_rys_int / dfb_rys_deriv need for this class and task count. */
 long dfb_rys_scratch_doubles(int la, int lb, int lc, long ntask, int deriv);
 
