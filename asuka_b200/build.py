@@ -30,14 +30,31 @@ def needs_build() -> bool:
     return any(os.path.getmtime(p) > t for p in deps if os.path.exists(p))
 
 
-def build(force: bool = False, verbose: bool = False) -> str:
+def build(force: bool = False, verbose: bool = False, jobs: int | None = None) -> str:
+    """Compile every csrc/*.cu to an object in parallel (they are independent), then link."""
     if not force and not needs_build():
         return OUT
     nvcc = os.environ.get("NVCC", "nvcc")
-    cmd = [nvcc, *NVCC_FLAGS, "-o", OUT + ".tmp", *sources()]
-    if verbose:
-        print(" ".join(cmd), flush=True)
-    subprocess.run(cmd, check=True, cwd=CSRC)
+    objdir = os.path.join(HERE, "_build")
+    os.makedirs(objdir, exist_ok=True)
+    compile_flags = [f for f in NVCC_FLAGS if f not in ("--shared", "-lcublas")]
+    procs = []
+    objs = []
+    jobs = jobs or max(1, os.cpu_count() or 1)
+    for src in sources():
+        obj = os.path.join(objdir, os.path.basename(src)[:-3] + ".o")
+        objs.append(obj)
+        cmd = [nvcc, *compile_flags, "-c", src, "-o", obj]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        while len([p for p in procs if p.poll() is None]) >= jobs:
+            procs[0].wait() if procs[0].poll() is None else procs.pop(0)
+        procs.append(subprocess.Popen(cmd, cwd=CSRC))
+    for p in procs:
+        if p.wait() != 0:
+            raise RuntimeError(f"nvcc failed: {p.args}")
+    subprocess.run([nvcc, "-gencode", "arch=compute_100a,code=sm_100a", "--shared", "-o", OUT + ".tmp", *objs],
+                   check=True, cwd=CSRC)
     os.replace(OUT + ".tmp", OUT)
     return OUT
 

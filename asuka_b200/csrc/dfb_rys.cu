@@ -27,10 +27,12 @@
 // per-call moment solver.
 
 #include <stdio.h>
+#include <stdlib.h>
 #include <string.h>
 
 #include "../../include/dfb.h"
 #include "dfb_common.cuh"
+#include "dfb_cls_dispatch.h"
 #include "dfb_internal.h"
 
 namespace dfb {
@@ -95,7 +97,7 @@ __device__ __forceinline__ int e_index(const ClassInfo& ci, int x, int y, int z)
     return ncart_below(L) - ncart_below(ci.lmin) + cart_index(x, y, L);
 }
 
-__constant__ double c_binom[DFB_LMAX + 2][DFB_LMAX + 2];
+__constant__ double c_binomtab[DFB_LMAX + 2][DFB_LMAX + 2];
 
 // (a b | f) = sum_k C(b,k) AB^(b-k) (a+k 0 | f), per direction, from E[e*nf + f].
 __device__ __forceinline__ double hrr(const ClassInfo& ci, const double* E, int ax, int ay, int az, int bx, int by,
@@ -103,13 +105,13 @@ __device__ __forceinline__ double hrr(const ClassInfo& ci, const double* E, int 
     double sum = 0.0;
     double px = 1.0;
     for (int kx = bx; kx >= 0; --kx) {
-        const double cx = c_binom[bx][kx] * px;
+        const double cx = c_binomtab[bx][kx] * px;
         double py = 1.0;
         for (int ky = by; ky >= 0; --ky) {
-            const double cxy = cx * c_binom[by][ky] * py;
+            const double cxy = cx * c_binomtab[by][ky] * py;
             double pz = 1.0;
             for (int kz = bz; kz >= 0; --kz) {
-                const double c = cxy * c_binom[bz][kz] * pz;
+                const double c = cxy * c_binomtab[bz][kz] * pz;
                 sum += c * E[e_index(ci, ax + kx, ay + ky, az + kz) * ci.nf + f];
                 pz *= AB[2];
             }
@@ -533,9 +535,39 @@ static int dispatch_rys(int la, int lb, int lc, const dfb_pair_side_t* ps, const
                 }
                 h[n][k] = v;
             }
-        cudaError_t e = cudaMemcpyToSymbol(c_binom, h, sizeof(h));
+        cudaError_t e = cudaMemcpyToSymbol(c_binomtab, h, sizeof(h));
         if (e != cudaSuccess) return set_cuda_error("binomial table upload", e);
         g_binom_ready[dev] = true;
+    }
+    if (!query_only && ntask > 0 && getenv("DFB_DISABLE_TMPL") == nullptr) {
+        TmplArgs g;
+        g.ps = *ps;
+        g.ax = *ax;
+        g.task_pair = task_pair;
+        g.task_aux = task_aux;
+        g.ntask = ntask;
+        g.naux_grid = naux_grid;
+        g.mode = mode;
+        g.out = out;
+        g.sP = sP;
+        g.sM = sM;
+        g.sN = sN;
+        g.bar = bar;
+        g.sbP = sbP;
+        g.sbM = sbM;
+        g.sbN = sbN;
+        g.grad = grad;
+        g.natm = natm;
+        g.smem_grad = (DERIV && natm * 3 <= 4096) ? 1 : 0;
+        g.tab = g_tables[dev].tab;
+        const size_t smem = g.smem_grad ? sizeof(double) * natm * 3 : 0;
+        const long nblk = (ntask + 127) / 128;
+        if (nblk > 2147483647L) return set_error(DFB_ERR_INVALID, "too many tasks in one class launch");
+        if (tmpl_launch(la, lb, lc, DERIV, g, nblk, smem, st)) {
+            cudaError_t e = cudaGetLastError();
+            if (e != cudaSuccess) return set_cuda_error("k_rys_thread launch", e);
+            return DFB_OK;
+        }
     }
     const int kb = (ci.nef + 31) / 32;
 #define DFB_CASE(K)                                                                                              \
@@ -561,6 +593,10 @@ extern "C" int dfb_rys_table_init(const double* coef, const int* offs, long ncoe
     clear_error();
     if (nmax < 1 || nmax > DFB_NROOTS_MAX || nint < 1 || deg < 0 || !coef || !herm || !offs || !hoffs)
         return set_error(DFB_ERR_INVALID, "invalid Rys table description");
+    if (deg != DFB_RYS_DEG)
+        return set_error(DFB_ERR_INVALID, "Rys table degree %d, kernels are compiled for %d", deg, DFB_RYS_DEG);
+    for (int n = 1; n <= nmax; ++n)
+        if (offs[n] % 2 != 0) return set_error(DFB_ERR_INVALID, "Rys table blocks must be 16-byte aligned");
     const int dev = current_device();
     DeviceTable& t = g_tables[dev];
     if (t.ready) return DFB_OK;

@@ -1,0 +1,440 @@
+// Class-specialised Rys kernels: one thread per (task, aux-component subset).
+//
+// For low and medium angular momenta the per-task work is dominated by the
+// primitive loop (root evaluation, 2D recurrences, accumulation), so each
+// thread owns one task -- an AB shell pair times one aux shell -- and keeps
+// the recurrence tables and the contracted intermediate (e 0|f) in registers.
+// LA, LB, LC, the root count and every loop bound are compile-time constants;
+// every Cartesian component index is a template argument (integer_sequence
+// folds), so all array indices are literal constants and the arrays live in
+// registers.  Classes whose intermediate does not fit are split over FS
+// threads, each owning a contiguous subset of the aux shell's Cartesian
+// components (subset = blockIdx.y, uniform per block).
+//
+// Consecutive threads hold consecutive aux shells of the same AB pair (the
+// task grid is pair-major and the aux list of a class is sorted by primitive
+// count), so the pair-table reads of a warp are broadcasts and the primitive
+// loops of a warp have similar trip counts.
+//
+// The derivative variant (DERIV) accumulates U = sum S, WA = sum 2a S and
+// WB = sum 2b S over |e| in [LA-1, LA+LB+1] per primitive triplet and contracts
+//   d/dA = 2a (a+1_d) - a_d (a-1_d),  d/dB = 2b [(a+1_d, b) + AB_d (a, b)] - b_d (a, b-1_d)
+// with the adjoint tile; d/dC = -(d/dA + d/dB) (translational invariance).
+#pragma once
+#include <utility>
+
+#include "../../include/dfb.h"
+#include "dfb_common.cuh"
+
+#define DFB_RYS_DEG 15  // Horner degree of the Rys table (checked at upload)
+
+namespace dfb {
+
+__host__ __device__ constexpr int c_ncart(int l) { return (l + 1) * (l + 2) / 2; }
+__host__ __device__ constexpr int c_ncb(int L) { return L * (L + 1) * (L + 2) / 6; }
+
+__host__ __device__ constexpr int c_cx(int l, int i) {
+    int x = l;
+    while (i > l - x) {
+        i -= (l - x + 1);
+        --x;
+    }
+    return x;
+}
+__host__ __device__ constexpr int c_cy(int l, int i) {
+    int x = l;
+    while (i > l - x) {
+        i -= (l - x + 1);
+        --x;
+    }
+    return l - x - i;
+}
+__host__ __device__ constexpr int c_cz(int l, int i) { return l - c_cx(l, i) - c_cy(l, i); }
+__host__ __device__ constexpr int c_eidx(int LMIN, int x, int y, int z) {
+    return c_ncb(x + y + z) - c_ncb(LMIN) + ((y + z) * (y + z + 1)) / 2 + z;
+}
+__host__ __device__ constexpr int c_eL(int LMIN, int e) {
+    int L = LMIN;
+    while (e >= c_ncart(L)) {
+        e -= c_ncart(L);
+        ++L;
+    }
+    return L;
+}
+__host__ __device__ constexpr int c_ex(int LMIN, int e) {
+    return c_cx(c_eL(LMIN, e), e - (c_ncb(c_eL(LMIN, e)) - c_ncb(LMIN)));
+}
+__host__ __device__ constexpr int c_ey(int LMIN, int e) {
+    return c_cy(c_eL(LMIN, e), e - (c_ncb(c_eL(LMIN, e)) - c_ncb(LMIN)));
+}
+__host__ __device__ constexpr int c_ez(int LMIN, int e) {
+    return c_cz(c_eL(LMIN, e), e - (c_ncb(c_eL(LMIN, e)) - c_ncb(LMIN)));
+}
+__host__ __device__ constexpr double c_binom(int n, int k) {
+    double v = 1.0;
+    for (int i = 1; i <= k; ++i) v = v * (double)(n - k + i) / (double)i;
+    return (k < 0 || k > n) ? 0.0 : v;
+}
+
+template <int NR>
+__device__ __forceinline__ void rys_eval_t(const RysTable& tab, double T, double (&x)[NR], double (&w)[NR]) {
+    if (T >= tab.tmax) {
+        const double* h = tab.herm + tab.hoff[NR];
+        const double inv = 1.0 / T;
+        const double rs = rsqrt(T);
+#pragma unroll
+        for (int i = 0; i < NR; ++i) {
+            x[i] = __ldg(h + i) * inv;
+            w[i] = __ldg(h + NR + i) * rs;
+        }
+        return;
+    }
+    int k = (int)T;
+    if (k > tab.nint - 1) k = tab.nint - 1;
+    const double u = 2.0 * (T - (double)k) - 1.0;
+    constexpr int S = DFB_RYS_DEG + 1;
+    const double2* c = reinterpret_cast<const double2*>(tab.coef + tab.offs[NR] + (size_t)k * (2 * NR) * S);
+#pragma unroll
+    for (int r = 0; r < 2 * NR; ++r) {
+        double cf[S];
+#pragma unroll
+        for (int d = 0; d < S / 2; ++d) {
+            const double2 v = __ldg(c + r * (S / 2) + d);
+            cf[2 * d] = v.x;
+            cf[2 * d + 1] = v.y;
+        }
+        double acc = cf[S - 1];
+#pragma unroll
+        for (int d = S - 2; d >= 0; --d) acc = fma(acc, u, cf[d]);
+        if (r < NR)
+            x[r] = acc;
+        else
+            w[r - NR] = acc;
+    }
+}
+
+template <int NM, int MM>
+__device__ __forceinline__ void build_G_t(double (&G)[NM + 1][MM + 1], double g00, double C, double Cp, double B0,
+                                          double B1, double B1p) {
+    G[0][0] = g00;
+#pragma unroll
+    for (int a = 1; a <= NM; ++a) {
+        double v = C * G[a - 1][0];
+        if (a >= 2) v += B1 * (double)(a - 1) * G[a >= 2 ? a - 2 : 0][0];
+        G[a][0] = v;
+    }
+#pragma unroll
+    for (int b = 1; b <= MM; ++b) {
+        double v = Cp * G[0][b - 1];
+        if (b >= 2) v += B1p * (double)(b - 1) * G[0][b >= 2 ? b - 2 : 0];
+        G[0][b] = v;
+    }
+#pragma unroll
+    for (int a = 1; a <= NM; ++a) {
+#pragma unroll
+        for (int b = 1; b <= MM; ++b) {
+            double v = (double)a * B0 * G[a - 1][b - 1] + Cp * G[a][b - 1];
+            if (b >= 2) v += B1p * (double)(b - 1) * G[a][b >= 2 ? b - 2 : 0];
+            G[a][b] = v;
+        }
+    }
+}
+
+struct TmplArgs {
+    dfb_pair_side_t ps;
+    dfb_aux_side_t ax;
+    const int* task_pair;
+    const int* task_aux;
+    long ntask;
+    long naux_grid;
+    int mode;
+    double* out;
+    long sP, sM, sN;
+    const double* bar;
+    long sbP, sbM, sbN;
+    double* grad;
+    int natm;
+    int smem_grad;
+    RysTable tab;
+};
+
+static constexpr double kTwoPi52_t = 2.0 * 3.141592653589793238462643383279502884 *
+                                     3.141592653589793238462643383279502884 * 1.772453850905516027298167483341145182;
+
+// Compile-time description of one class and one component subset.
+template <int LA_, int LB_, int LC_, int FS_, int FSI_, bool DERIV_>
+struct Cls {
+    static constexpr int LA = LA_, LB = LB_, LC = LC_, FS = FS_, FSI = FSI_;
+    static constexpr bool DERIV = DERIV_;
+    static constexpr int NR = (LA + LB + LC + (DERIV ? 1 : 0)) / 2 + 1;
+    static constexpr int NM = LA + LB + (DERIV ? 1 : 0);
+    static constexpr int MM = LC;
+    static constexpr int LMIN = DERIV ? (LA > 0 ? LA - 1 : 0) : LA;
+    static constexpr int NE = c_ncb(NM + 1) - c_ncb(LMIN);
+    static constexpr int NF = c_ncart(LC);
+    static constexpr int NFS = (NF + FS - 1) / FS;
+    static constexpr int F0 = FSI * NFS;
+    static constexpr int F1 = (F0 + NFS < NF) ? (F0 + NFS) : NF;
+    static constexpr int NL = F1 - F0;
+    static constexpr int NA = c_ncart(LA), NB = c_ncart(LB);
+    static constexpr int NW = DERIV ? 3 : 1;
+    typedef double Acc[NW][NE][NL];
+    typedef double Gt[NM + 1][MM + 1];
+    typedef double ABt[3][LB + 2];
+
+    // accumulate element K = e*NL + f for one root
+    template <int K>
+    __device__ __forceinline__ static void acc_one(Acc& acc, const Gt& Gx, const Gt& Gy, const Gt& Gz, double a2,
+                                                   double b2) {
+        constexpr int e = K / NL, f = K % NL;
+        constexpr int ex = c_ex(LMIN, e), ey = c_ey(LMIN, e), ez = c_ez(LMIN, e);
+        constexpr int fx = c_cx(LC, F0 + f), fy = c_cy(LC, F0 + f), fz = c_cz(LC, F0 + f);
+        const double t = Gx[ex][fx] * Gy[ey][fy] * Gz[ez][fz];
+        acc[0][e][f] += t;
+        if constexpr (DERIV) {
+            acc[1 % NW][e][f] = fma(a2, t, acc[1 % NW][e][f]);
+            acc[2 % NW][e][f] = fma(b2, t, acc[2 % NW][e][f]);
+        }
+    }
+    template <int... Ks>
+    __device__ __forceinline__ static void acc_all(Acc& acc, const Gt& Gx, const Gt& Gy, const Gt& Gz, double a2,
+                                                   double b2, std::integer_sequence<int, Ks...>) {
+        (acc_one<Ks>(acc, Gx, Gy, Gz, a2, b2), ...);
+    }
+
+    // binomial coefficient with compile-time arguments
+    template <int N, int K>
+    struct Binom {
+        static constexpr double value = c_binom(N, K);
+    };
+
+    // (a b | f) from accumulator W, all indices compile-time
+    template <int W, int AX, int AY, int AZ, int BX, int BY, int BZ, int F, int KX, int KY, int KZ>
+    __device__ __forceinline__ static double hrr_term(const Acc& acc, const ABt& ABp) {
+        constexpr double c = Binom<BX, KX>::value * Binom<BY, KY>::value * Binom<BZ, KZ>::value;
+        constexpr int idx = c_eidx(LMIN, AX + KX, AY + KY, AZ + KZ);
+        return c * ABp[0][BX - KX] * ABp[1][BY - KY] * ABp[2][BZ - KZ] * acc[W][idx][F];
+    }
+    template <int W, int AX, int AY, int AZ, int BX, int BY, int BZ, int F, int... Ks>
+    __device__ __forceinline__ static double hrr_sum(const Acc& acc, const ABt& ABp, std::integer_sequence<int, Ks...>) {
+        constexpr int NYZ = (BY + 1) * (BZ + 1);
+        return (hrr_term<W, AX, AY, AZ, BX, BY, BZ, F, Ks / NYZ, (Ks / (BZ + 1)) % (BY + 1), Ks % (BZ + 1)>(acc, ABp) +
+                ...);
+    }
+    template <int W, int AX, int AY, int AZ, int BX, int BY, int BZ, int F>
+    __device__ __forceinline__ static double hrr(const Acc& acc, const ABt& ABp) {
+        return hrr_sum<W, AX, AY, AZ, BX, BY, BZ, F>(
+            acc, ABp, std::make_integer_sequence<int, (BX + 1) * (BY + 1) * (BZ + 1)>{});
+    }
+
+    // output element K = (ia*NB + ib)*NL + f
+    template <int K>
+    __device__ __forceinline__ static void out_one(const Acc& acc, const ABt& ABp, const TmplArgs& g, long aoA,
+                                                   long aoB, long aoC) {
+        constexpr int f = K % NL, ib = (K / NL) % NB, ia = K / (NL * NB);
+        constexpr int ax = c_cx(LA, ia), ay = c_cy(LA, ia), az = c_cz(LA, ia);
+        constexpr int bx = c_cx(LB, ib), by = c_cy(LB, ib), bz = c_cz(LB, ib);
+        const double v = hrr<0, ax, ay, az, bx, by, bz, f>(acc, ABp);
+        const long P = aoC + F0 + f, mu = aoA + ia, nu = aoB + ib;
+        if (g.mode == 0) {
+            g.out[P * g.sP + mu * g.sM + nu * g.sN] = v;
+            g.out[P * g.sP + nu * g.sM + mu * g.sN] = v;
+        } else {
+            g.out[P * g.sP + mu * g.sM] = v;
+            g.out[mu * g.sP + P * g.sM] = v;
+        }
+    }
+    template <int... Ks>
+    __device__ __forceinline__ static void out_all(const Acc& acc, const ABt& ABp, const TmplArgs& g, long aoA,
+                                                   long aoB, long aoC, std::integer_sequence<int, Ks...>) {
+        (out_one<Ks>(acc, ABp, g, aoA, aoB, aoC), ...);
+    }
+
+    // derivative contraction of element K with the adjoint, direction D
+    template <int K, int D>
+    __device__ __forceinline__ static void der_dir(const Acc& acc, const ABt& ABp, const double* AB, double gam,
+                                                   double (&gA)[3], double (&gB)[3], bool bdummy) {
+        constexpr int f = K % NL, ib = (K / NL) % NB, ia = K / (NL * NB);
+        constexpr int ax = c_cx(LA, ia), ay = c_cy(LA, ia), az = c_cz(LA, ia);
+        constexpr int bx = c_cx(LB, ib), by = c_cy(LB, ib), bz = c_cz(LB, ib);
+        constexpr int ad = D == 0 ? ax : (D == 1 ? ay : az);
+        constexpr int bd = D == 0 ? bx : (D == 1 ? by : bz);
+        constexpr int px = ax + (D == 0), py = ay + (D == 1), pz = az + (D == 2);
+        double dA = hrr<1, px, py, pz, bx, by, bz, f>(acc, ABp);
+        if constexpr (ad > 0)
+            dA -= (double)ad * hrr<0, ax - (D == 0), ay - (D == 1), az - (D == 2), bx, by, bz, f>(acc, ABp);
+        gA[D] = fma(gam, dA, gA[D]);
+        if (!bdummy) {
+            double dB =
+                hrr<2, px, py, pz, bx, by, bz, f>(acc, ABp) + AB[D] * hrr<2, ax, ay, az, bx, by, bz, f>(acc, ABp);
+            if constexpr (bd > 0)
+                dB -= (double)bd * hrr<0, ax, ay, az, bx - (D == 0), by - (D == 1), bz - (D == 2), f>(acc, ABp);
+            gB[D] = fma(gam, dB, gB[D]);
+        }
+    }
+    template <int K>
+    __device__ __forceinline__ static void der_one(const Acc& acc, const ABt& ABp, const double* AB,
+                                                   const TmplArgs& g, long aoA, long aoB, long aoC, double (&gA)[3],
+                                                   double (&gB)[3]) {
+        constexpr int f = K % NL, ib = (K / NL) % NB, ia = K / (NL * NB);
+        double gam;
+        if (g.mode == 0)
+            gam = g.bar[(aoC + F0 + f) * g.sbP + (aoA + ia) * g.sbM + (aoB + ib) * g.sbN];
+        else
+            gam = g.bar[(aoA + ia) * g.sbP + (aoC + F0 + f) * g.sbM];
+        der_dir<K, 0>(acc, ABp, AB, gam, gA, gB, g.ps.b_dummy);
+        der_dir<K, 1>(acc, ABp, AB, gam, gA, gB, g.ps.b_dummy);
+        der_dir<K, 2>(acc, ABp, AB, gam, gA, gB, g.ps.b_dummy);
+    }
+    template <int... Ks>
+    __device__ __forceinline__ static void der_all(const Acc& acc, const ABt& ABp, const double* AB,
+                                                   const TmplArgs& g, long aoA, long aoB, long aoC, double (&gA)[3],
+                                                   double (&gB)[3], std::integer_sequence<int, Ks...>) {
+        (der_one<Ks>(acc, ABp, AB, g, aoA, aoB, aoC, gA, gB), ...);
+    }
+};
+
+template <class CL>
+__device__ __forceinline__ void rys_thread_body(const TmplArgs& g, long task, double* sgrad) {
+    constexpr int NR = CL::NR, NM = CL::NM, MM = CL::MM, LB = CL::LB;
+    const long tp = g.naux_grid > 0 ? task / g.naux_grid : task;
+    const long ta = g.naux_grid > 0 ? task - tp * g.naux_grid : task;
+    const int pair = g.task_pair[tp];
+    const int C = g.task_aux[ta];
+    const int shA = g.ps.shA[pair];
+    const int shB = g.ps.b_dummy ? -1 : g.ps.shB[pair];
+    double A[3], AB[3], Cc[3];
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        A[d] = g.ps.cxyz[3 * shA + d];
+        const double Bd = g.ps.b_dummy ? 0.0 : g.ps.cxyz[3 * shB + d];
+        AB[d] = A[d] - Bd;
+        Cc[d] = g.ax.cxyz[3 * C + d];
+    }
+    const int p0 = g.ps.pstart[pair];
+    const int nab = g.ps.npair[pair];
+    const int c0 = g.ax.pstart[C];
+    const int nc = g.ax.nprim[C];
+
+    typename CL::Acc acc;
+#pragma unroll
+    for (int w = 0; w < CL::NW; ++w)
+#pragma unroll
+        for (int e = 0; e < CL::NE; ++e)
+#pragma unroll
+            for (int f = 0; f < CL::NL; ++f) acc[w][e][f] = 0.0;
+
+    for (int iab = 0; iab < nab; ++iab) {
+        const double p = g.ps.eta[p0 + iab];
+        const double cK = g.ps.cK[p0 + iab];
+        const double a2 = CL::DERIV ? 2.0 * g.ps.ea[p0 + iab] : 0.0;
+        const double b2 = CL::DERIV ? 2.0 * g.ps.eb[p0 + iab] : 0.0;
+        const double Pp[3] = {g.ps.Px[p0 + iab], g.ps.Py[p0 + iab], g.ps.Pz[p0 + iab]};
+        double PA[3], CP[3], PQ2 = 0.0;
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            PA[d] = Pp[d] - A[d];
+            CP[d] = Cc[d] - Pp[d];
+            PQ2 += CP[d] * CP[d];
+        }
+        for (int ic = 0; ic < nc; ++ic) {
+            const double q = g.ax.pexp[c0 + ic];
+            const double cc = g.ax.pcoef[c0 + ic];
+            const double inv = 1.0 / (p + q);
+            const double T = p * q * inv * PQ2;
+            const double pref = kTwoPi52_t / (p * q * sqrt(p + q)) * cK * cc;
+            double xr[NR], wr[NR];
+            rys_eval_t<NR>(g.tab, T, xr, wr);
+            const double qi = q * inv, pi = p * inv;
+            const double h_p = 0.5 / p, h_q = 0.5 / q;
+#pragma unroll
+            for (int u = 0; u < NR; ++u) {
+                const double x = xr[u];
+                const double B0 = x * 0.5 * inv;
+                const double B1 = (1.0 - x) * h_p + B0;
+                const double B1p = (1.0 - x) * h_q + B0;
+                typename CL::Gt Gx, Gy, Gz;
+                build_G_t<NM, MM>(Gx, pref * wr[u], PA[0] + qi * x * CP[0], -pi * x * CP[0], B0, B1, B1p);
+                build_G_t<NM, MM>(Gy, 1.0, PA[1] + qi * x * CP[1], -pi * x * CP[1], B0, B1, B1p);
+                build_G_t<NM, MM>(Gz, 1.0, PA[2] + qi * x * CP[2], -pi * x * CP[2], B0, B1, B1p);
+                CL::acc_all(acc, Gx, Gy, Gz, a2, b2, std::make_integer_sequence<int, CL::NE * CL::NL>{});
+            }
+        }
+    }
+
+    typename CL::ABt ABp;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        ABp[d][0] = 1.0;
+#pragma unroll
+        for (int k = 1; k < LB + 2; ++k) ABp[d][k] = ABp[d][k - 1] * AB[d];
+    }
+    const long aoA = g.ps.aostart[shA];
+    const long aoB = g.ps.b_dummy ? 0 : g.ps.aostart[shB];
+    const long aoC = g.ax.aostart[C];
+    constexpr int NOUT = CL::NA * CL::NB * CL::NL;
+    if constexpr (!CL::DERIV) {
+        CL::out_all(acc, ABp, g, aoA, aoB, aoC, std::make_integer_sequence<int, NOUT>{});
+    } else {
+        double gA[3] = {0.0, 0.0, 0.0}, gB[3] = {0.0, 0.0, 0.0};
+        CL::der_all(acc, ABp, AB, g, aoA, aoB, aoC, gA, gB, std::make_integer_sequence<int, NOUT>{});
+        const bool offdiag = (g.mode == 0) ? (shA != shB) : (shA != C);
+        const double fac = offdiag ? 2.0 : 1.0;
+        const int atA = g.ps.atom[shA];
+        const int atB = g.ps.b_dummy ? -1 : g.ps.atom[shB];
+        const int atC = g.ax.atom[C];
+        double* G = g.smem_grad ? sgrad : g.grad;
+#pragma unroll
+        for (int d = 0; d < 3; ++d) {
+            const double vA = fac * gA[d], vB = fac * gB[d];
+            atomicAdd(G + 3 * atA + d, vA);
+            if (atB >= 0) atomicAdd(G + 3 * atB + d, vB);
+            atomicAdd(G + 3 * atC + d, -(vA + vB));
+        }
+    }
+}
+
+template <int LA, int LB, int LC, int FS, bool DERIV>
+__global__ void __launch_bounds__(128) k_rys_thread(TmplArgs g) {
+    extern __shared__ double sgrad[];
+    const int ng = (DERIV && g.smem_grad) ? g.natm * 3 : 0;
+    if (DERIV && g.smem_grad) {
+        for (int i = threadIdx.x; i < ng; i += blockDim.x) sgrad[i] = 0.0;
+        __syncthreads();
+    }
+    const long task = (long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (task < g.ntask) {
+        switch (blockIdx.y) {
+#define DFB_FSI(I)                                                                                            \
+    case I:                                                                                                   \
+        if constexpr (I < FS) rys_thread_body<Cls<LA, LB, LC, FS, (I < FS ? I : 0), DERIV>>(g, task, sgrad); \
+        break;
+            DFB_FSI(0)
+            DFB_FSI(1)
+            DFB_FSI(2)
+            DFB_FSI(3)
+            DFB_FSI(4)
+            DFB_FSI(5)
+            DFB_FSI(6)
+            DFB_FSI(7)
+            DFB_FSI(8)
+            DFB_FSI(9)
+            DFB_FSI(10)
+            DFB_FSI(11)
+            DFB_FSI(12)
+            DFB_FSI(13)
+            DFB_FSI(14)
+            DFB_FSI(15)
+#undef DFB_FSI
+            default:
+                break;
+        }
+    }
+    if (DERIV && g.smem_grad) {
+        __syncthreads();
+        for (int i = threadIdx.x; i < ng; i += blockDim.x)
+            if (sgrad[i] != 0.0) atomicAdd(g.grad + i, sgrad[i]);
+    }
+}
+
+}  // namespace dfb

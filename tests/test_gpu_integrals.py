@@ -111,3 +111,28 @@ def test_derivative_contractions_match_oracle(name):
     assert np.abs(G2 - g2).max() <= 1e-11 * np.abs(g2).max()
     # translational invariance of each contraction
     assert np.abs(G3.sum(0)).max() <= 1e-10 * np.abs(g3).max()
+
+
+def test_specialised_and_generic_kernels_agree(monkeypatch):
+    """The class-specialised thread kernels and the generic warp kernel give the same tiles and gradients."""
+    g = golden("h2o_matzvp")
+    ao, aux, sp = bases_of(g)
+    eng = _engine(ao, aux)
+    natm = len(g["elements"])
+    X1 = eng.int3c("Qmn").clone()
+    V1 = eng.metric().clone()
+    rng = np.random.default_rng(3)
+    bar = torch.as_tensor(rng.standard_normal(tuple(X1.shape)), device="cuda")
+    bar = bar + bar.transpose(1, 2)
+    g1 = torch.zeros((natm, 3), dtype=torch.float64, device="cuda")
+    eng.deriv3c(bar, g1)
+    monkeypatch.setenv("DFB_DISABLE_TMPL", "1")
+    X2 = eng.int3c("Qmn")
+    V2 = eng.metric()
+    g2 = torch.zeros_like(g1)
+    eng.deriv3c(bar, g2)
+    monkeypatch.delenv("DFB_DISABLE_TMPL")
+    sx = float(X2.abs().max())
+    assert float((X1 - X2).abs().max()) <= 1e-13 * sx
+    assert float((V1 - V2).abs().max()) <= 1e-13 * float(V2.abs().max())
+    assert float((g1 - g2).abs().max()) <= 1e-11 * float(g2.abs().max())
