@@ -161,80 +161,147 @@ struct TmplArgs {
 static constexpr double kTwoPi52_t = 2.0 * 3.141592653589793238462643383279502884 *
                                      3.141592653589793238462643383279502884 * 1.772453850905516027298167483341145182;
 
-// Compile-time description of one class and one component subset.
-template <int LA_, int LB_, int LC_, int FS_, int FSI_, bool DERIV_>
+// Compile-time description of one class, one component subset and one pass.
+//   MODE 0: integrals            one accumulator  E  over |e| in [LA, LA+LB]
+//   MODE 1: derivative, combined U, WA, WB        over |e| in [LA-1, LA+LB+1]
+//   MODE 2: derivative, centre A U  over [LA-1, LA+LB-1], WA over [LA+1, LA+LB+1]
+//   MODE 3: derivative, centre B U  over [LA, LA+LB-1],   WB over [LA, LA+LB+1]
+// Centre C gets -(A + B) from the pass(es) that computed them.
+template <int LA_, int LB_, int LC_, int FS_, int FSI_, int MODE_>
 struct Cls {
-    static constexpr int LA = LA_, LB = LB_, LC = LC_, FS = FS_, FSI = FSI_;
-    static constexpr bool DERIV = DERIV_;
+    static constexpr int LA = LA_, LB = LB_, LC = LC_, FS = FS_, FSI = FSI_, MODE = MODE_;
+    static constexpr bool DERIV = MODE > 0;
     static constexpr int NR = (LA + LB + LC + (DERIV ? 1 : 0)) / 2 + 1;
     static constexpr int NM = LA + LB + (DERIV ? 1 : 0);
-    static constexpr int MM = LC;
-    static constexpr int LMIN = DERIV ? (LA > 0 ? LA - 1 : 0) : LA;
-    static constexpr int NE = c_ncb(NM + 1) - c_ncb(LMIN);
     static constexpr int NF = c_ncart(LC);
     static constexpr int NFS = (NF + FS - 1) / FS;
     static constexpr int F0 = FSI * NFS;
     static constexpr int F1 = (F0 + NFS < NF) ? (F0 + NFS) : NF;
     static constexpr int NL = F1 - F0;
     static constexpr int NA = c_ncart(LA), NB = c_ncart(LB);
-    static constexpr int NW = DERIV ? 3 : 1;
-    typedef double Acc[NW][NE][NL];
-    typedef double Gt[NM + 1][MM + 1];
+    static constexpr int NARR = MODE == 0 ? 1 : (MODE == 1 ? 3 : 2);
+    __host__ __device__ static constexpr int lo(int k) {
+        return MODE == 0 ? LA
+             : MODE == 1 ? (LA > 0 ? LA - 1 : 0)
+             : MODE == 2 ? (k == 0 ? (LA > 0 ? LA - 1 : 0) : LA + 1)
+                         : LA;
+    }
+    __host__ __device__ static constexpr int hi(int k) {
+        return MODE == 0 ? LA + LB
+             : MODE == 1 ? NM
+             : MODE == 2 ? (k == 0 ? (LA > 0 ? LA + LB - 1 : -1) : LA + LB + 1)
+                         : (k == 0 ? LA + LB - 1 : LA + LB + 1);
+    }
+    // weight of array k: 0 -> 1, 1 -> 2a, 2 -> 2b
+    __host__ __device__ static constexpr int wt(int k) { return MODE == 1 ? k : (MODE == 2 ? (k == 0 ? 0 : 1) : (k == 0 ? 0 : 2)); }
+    __host__ __device__ static constexpr int ne(int k) { return (k < NARR && hi(k) >= lo(k)) ? c_ncb(hi(k) + 1) - c_ncb(lo(k)) : 0; }
+    static constexpr int NE0 = ne(0) > 0 ? ne(0) : 1, NE1 = ne(1) > 0 ? ne(1) : 1, NE2 = ne(2) > 0 ? ne(2) : 1;
+    __host__ __device__ static constexpr int md(int d) {
+        int m = 0;
+        for (int f = F0; f < F1; ++f) {
+            const int v = d == 0 ? c_cx(LC, f) : (d == 1 ? c_cy(LC, f) : c_cz(LC, f));
+            m = v > m ? v : m;
+        }
+        return m;
+    }
+    static constexpr int MDX = md(0), MDY = md(1), MDZ = md(2);
+    struct Acc {
+        double a0[NE0][NL];
+        double a1[NE1][NL];
+        double a2[NE2][NL];
+    };
+    typedef double GtX[NM + 1][MDX + 1];
+    typedef double GtY[NM + 1][MDY + 1];
+    typedef double GtZ[NM + 1][MDZ + 1];
     typedef double ABt[3][LB + 2];
 
-    // accumulate element K = e*NL + f for one root
     template <int K>
-    __device__ __forceinline__ static void acc_one(Acc& acc, const Gt& Gx, const Gt& Gy, const Gt& Gz, double a2,
-                                                   double b2) {
-        constexpr int e = K / NL, f = K % NL;
-        constexpr int ex = c_ex(LMIN, e), ey = c_ey(LMIN, e), ez = c_ez(LMIN, e);
-        constexpr int fx = c_cx(LC, F0 + f), fy = c_cy(LC, F0 + f), fz = c_cz(LC, F0 + f);
-        const double t = Gx[ex][fx] * Gy[ey][fy] * Gz[ez][fz];
-        acc[0][e][f] += t;
-        if constexpr (DERIV) {
-            acc[1 % NW][e][f] = fma(a2, t, acc[1 % NW][e][f]);
-            acc[2 % NW][e][f] = fma(b2, t, acc[2 % NW][e][f]);
-        }
+    __device__ __forceinline__ static double& at(Acc& A, int e, int f) {
+        if constexpr (K == 0) return A.a0[e][f];
+        else if constexpr (K == 1) return A.a1[e][f];
+        else return A.a2[e][f];
     }
-    template <int... Ks>
-    __device__ __forceinline__ static void acc_all(Acc& acc, const Gt& Gx, const Gt& Gy, const Gt& Gz, double a2,
-                                                   double b2, std::integer_sequence<int, Ks...>) {
-        (acc_one<Ks>(acc, Gx, Gy, Gz, a2, b2), ...);
+    template <int K>
+    __device__ __forceinline__ static double get(const Acc& A, int e, int f) {
+        if constexpr (K == 0) return A.a0[e][f];
+        else if constexpr (K == 1) return A.a1[e][f];
+        else return A.a2[e][f];
     }
 
-    // binomial coefficient with compile-time arguments
+    // accumulate element J = e*NL + f of array K for one root
+    template <int K, int J>
+    __device__ __forceinline__ static void acc_one(Acc& A, const GtX& Gx, const GtY& Gy, const GtZ& Gz, double a2,
+                                                   double b2) {
+        constexpr int e = J / NL, f = J % NL;
+        constexpr int ex = c_ex(lo(K), e), ey = c_ey(lo(K), e), ez = c_ez(lo(K), e);
+        constexpr int fx = c_cx(LC, F0 + f), fy = c_cy(LC, F0 + f), fz = c_cz(LC, F0 + f);
+        const double t = Gx[ex][fx] * Gy[ey][fy] * Gz[ez][fz];
+        if constexpr (wt(K) == 0)
+            at<K>(A, e, f) += t;
+        else if constexpr (wt(K) == 1)
+            at<K>(A, e, f) = fma(a2, t, at<K>(A, e, f));
+        else
+            at<K>(A, e, f) = fma(b2, t, at<K>(A, e, f));
+    }
+    template <int K, int... Js>
+    __device__ __forceinline__ static void acc_arr(Acc& A, const GtX& Gx, const GtY& Gy, const GtZ& Gz, double a2,
+                                                   double b2, std::integer_sequence<int, Js...>) {
+        (acc_one<K, Js>(A, Gx, Gy, Gz, a2, b2), ...);
+    }
+    __device__ __forceinline__ static void acc_all(Acc& A, const GtX& Gx, const GtY& Gy, const GtZ& Gz, double a2,
+                                                   double b2) {
+        acc_arr<0>(A, Gx, Gy, Gz, a2, b2, std::make_integer_sequence<int, ne(0) * NL>{});
+        if constexpr (NARR > 1) acc_arr<1>(A, Gx, Gy, Gz, a2, b2, std::make_integer_sequence<int, ne(1) * NL>{});
+        if constexpr (NARR > 2) acc_arr<2>(A, Gx, Gy, Gz, a2, b2, std::make_integer_sequence<int, ne(2) * NL>{});
+    }
+    __device__ __forceinline__ static void zero(Acc& A) {
+#pragma unroll
+        for (int e = 0; e < NE0; ++e)
+#pragma unroll
+            for (int f = 0; f < NL; ++f) A.a0[e][f] = 0.0;
+#pragma unroll
+        for (int e = 0; e < NE1; ++e)
+#pragma unroll
+            for (int f = 0; f < NL; ++f) A.a1[e][f] = 0.0;
+#pragma unroll
+        for (int e = 0; e < NE2; ++e)
+#pragma unroll
+            for (int f = 0; f < NL; ++f) A.a2[e][f] = 0.0;
+    }
+
     template <int N, int K>
     struct Binom {
         static constexpr double value = c_binom(N, K);
     };
 
-    // (a b | f) from accumulator W, all indices compile-time
-    template <int W, int AX, int AY, int AZ, int BX, int BY, int BZ, int F, int KX, int KY, int KZ>
-    __device__ __forceinline__ static double hrr_term(const Acc& acc, const ABt& ABp) {
+    // (a b | f) from array K, all indices compile-time
+    template <int K, int AX, int AY, int AZ, int BX, int BY, int BZ, int F, int KX, int KY, int KZ>
+    __device__ __forceinline__ static double hrr_term(const Acc& A, const ABt& ABp) {
         constexpr double c = Binom<BX, KX>::value * Binom<BY, KY>::value * Binom<BZ, KZ>::value;
-        constexpr int idx = c_eidx(LMIN, AX + KX, AY + KY, AZ + KZ);
-        return c * ABp[0][BX - KX] * ABp[1][BY - KY] * ABp[2][BZ - KZ] * acc[W][idx][F];
+        constexpr int idx = c_eidx(lo(K), AX + KX, AY + KY, AZ + KZ);
+        static_assert(idx >= 0 && idx < ne(K), "horizontal recurrence reads outside the accumulated range");
+        return c * ABp[0][BX - KX] * ABp[1][BY - KY] * ABp[2][BZ - KZ] * get<K>(A, idx, F);
     }
-    template <int W, int AX, int AY, int AZ, int BX, int BY, int BZ, int F, int... Ks>
-    __device__ __forceinline__ static double hrr_sum(const Acc& acc, const ABt& ABp, std::integer_sequence<int, Ks...>) {
+    template <int K, int AX, int AY, int AZ, int BX, int BY, int BZ, int F, int... Ks>
+    __device__ __forceinline__ static double hrr_sum(const Acc& A, const ABt& ABp, std::integer_sequence<int, Ks...>) {
         constexpr int NYZ = (BY + 1) * (BZ + 1);
-        return (hrr_term<W, AX, AY, AZ, BX, BY, BZ, F, Ks / NYZ, (Ks / (BZ + 1)) % (BY + 1), Ks % (BZ + 1)>(acc, ABp) +
+        return (hrr_term<K, AX, AY, AZ, BX, BY, BZ, F, Ks / NYZ, (Ks / (BZ + 1)) % (BY + 1), Ks % (BZ + 1)>(A, ABp) +
                 ...);
     }
-    template <int W, int AX, int AY, int AZ, int BX, int BY, int BZ, int F>
-    __device__ __forceinline__ static double hrr(const Acc& acc, const ABt& ABp) {
-        return hrr_sum<W, AX, AY, AZ, BX, BY, BZ, F>(
-            acc, ABp, std::make_integer_sequence<int, (BX + 1) * (BY + 1) * (BZ + 1)>{});
+    template <int K, int AX, int AY, int AZ, int BX, int BY, int BZ, int F>
+    __device__ __forceinline__ static double hrr(const Acc& A, const ABt& ABp) {
+        return hrr_sum<K, AX, AY, AZ, BX, BY, BZ, F>(
+            A, ABp, std::make_integer_sequence<int, (BX + 1) * (BY + 1) * (BZ + 1)>{});
     }
 
-    // output element K = (ia*NB + ib)*NL + f
-    template <int K>
-    __device__ __forceinline__ static void out_one(const Acc& acc, const ABt& ABp, const TmplArgs& g, long aoA,
+    // output element J = (ia*NB + ib)*NL + f
+    template <int J>
+    __device__ __forceinline__ static void out_one(const Acc& A, const ABt& ABp, const TmplArgs& g, long aoA,
                                                    long aoB, long aoC) {
-        constexpr int f = K % NL, ib = (K / NL) % NB, ia = K / (NL * NB);
+        constexpr int f = J % NL, ib = (J / NL) % NB, ia = J / (NL * NB);
         constexpr int ax = c_cx(LA, ia), ay = c_cy(LA, ia), az = c_cz(LA, ia);
         constexpr int bx = c_cx(LB, ib), by = c_cy(LB, ib), bz = c_cz(LB, ib);
-        const double v = hrr<0, ax, ay, az, bx, by, bz, f>(acc, ABp);
+        const double v = hrr<0, ax, ay, az, bx, by, bz, f>(A, ABp);
         const long P = aoC + F0 + f, mu = aoA + ia, nu = aoB + ib;
         if (g.mode == 0) {
             g.out[P * g.sP + mu * g.sM + nu * g.sN] = v;
@@ -244,65 +311,72 @@ struct Cls {
             g.out[mu * g.sP + P * g.sM] = v;
         }
     }
-    template <int... Ks>
-    __device__ __forceinline__ static void out_all(const Acc& acc, const ABt& ABp, const TmplArgs& g, long aoA,
-                                                   long aoB, long aoC, std::integer_sequence<int, Ks...>) {
-        (out_one<Ks>(acc, ABp, g, aoA, aoB, aoC), ...);
+    template <int... Js>
+    __device__ __forceinline__ static void out_all(const Acc& A, const ABt& ABp, const TmplArgs& g, long aoA,
+                                                   long aoB, long aoC, std::integer_sequence<int, Js...>) {
+        (out_one<Js>(A, ABp, g, aoA, aoB, aoC), ...);
     }
 
-    // derivative contraction of element K with the adjoint, direction D
-    template <int K, int D>
-    __device__ __forceinline__ static void der_dir(const Acc& acc, const ABt& ABp, const double* AB, double gam,
+    // derivative of element J contracted with its adjoint value, direction D
+    template <int J, int D>
+    __device__ __forceinline__ static void der_dir(const Acc& A, const ABt& ABp, const double* AB, double gam,
                                                    double (&gA)[3], double (&gB)[3], bool bdummy) {
-        constexpr int f = K % NL, ib = (K / NL) % NB, ia = K / (NL * NB);
+        constexpr int f = J % NL, ib = (J / NL) % NB, ia = J / (NL * NB);
         constexpr int ax = c_cx(LA, ia), ay = c_cy(LA, ia), az = c_cz(LA, ia);
         constexpr int bx = c_cx(LB, ib), by = c_cy(LB, ib), bz = c_cz(LB, ib);
         constexpr int ad = D == 0 ? ax : (D == 1 ? ay : az);
         constexpr int bd = D == 0 ? bx : (D == 1 ? by : bz);
         constexpr int px = ax + (D == 0), py = ay + (D == 1), pz = az + (D == 2);
-        double dA = hrr<1, px, py, pz, bx, by, bz, f>(acc, ABp);
-        if constexpr (ad > 0)
-            dA -= (double)ad * hrr<0, ax - (D == 0), ay - (D == 1), az - (D == 2), bx, by, bz, f>(acc, ABp);
-        gA[D] = fma(gam, dA, gA[D]);
-        if (!bdummy) {
-            double dB =
-                hrr<2, px, py, pz, bx, by, bz, f>(acc, ABp) + AB[D] * hrr<2, ax, ay, az, bx, by, bz, f>(acc, ABp);
-            if constexpr (bd > 0)
-                dB -= (double)bd * hrr<0, ax, ay, az, bx - (D == 0), by - (D == 1), bz - (D == 2), f>(acc, ABp);
-            gB[D] = fma(gam, dB, gB[D]);
+        if constexpr (MODE == 1 || MODE == 2) {
+            constexpr int KW = MODE == 1 ? 1 : 1;  // WA
+            double dA = hrr<KW, px, py, pz, bx, by, bz, f>(A, ABp);
+            if constexpr (ad > 0)
+                dA -= (double)ad * hrr<0, ax - (D == 0), ay - (D == 1), az - (D == 2), bx, by, bz, f>(A, ABp);
+            gA[D] = fma(gam, dA, gA[D]);
+        }
+        if constexpr (MODE == 1 || MODE == 3) {
+            if (!bdummy) {
+                constexpr int KW = MODE == 1 ? 2 : 1;  // WB
+                double dB = hrr<KW, px, py, pz, bx, by, bz, f>(A, ABp) +
+                            AB[D] * hrr<KW, ax, ay, az, bx, by, bz, f>(A, ABp);
+                if constexpr (bd > 0)
+                    dB -= (double)bd * hrr<0, ax, ay, az, bx - (D == 0), by - (D == 1), bz - (D == 2), f>(A, ABp);
+                gB[D] = fma(gam, dB, gB[D]);
+            }
         }
     }
-    template <int K>
-    __device__ __forceinline__ static void der_one(const Acc& acc, const ABt& ABp, const double* AB,
+    template <int J>
+    __device__ __forceinline__ static void der_one(const Acc& A, const ABt& ABp, const double* AB,
                                                    const TmplArgs& g, long aoA, long aoB, long aoC, double (&gA)[3],
                                                    double (&gB)[3]) {
-        constexpr int f = K % NL, ib = (K / NL) % NB, ia = K / (NL * NB);
+        constexpr int f = J % NL, ib = (J / NL) % NB, ia = J / (NL * NB);
         double gam;
         if (g.mode == 0)
             gam = g.bar[(aoC + F0 + f) * g.sbP + (aoA + ia) * g.sbM + (aoB + ib) * g.sbN];
         else
             gam = g.bar[(aoA + ia) * g.sbP + (aoC + F0 + f) * g.sbM];
-        der_dir<K, 0>(acc, ABp, AB, gam, gA, gB, g.ps.b_dummy);
-        der_dir<K, 1>(acc, ABp, AB, gam, gA, gB, g.ps.b_dummy);
-        der_dir<K, 2>(acc, ABp, AB, gam, gA, gB, g.ps.b_dummy);
+        der_dir<J, 0>(A, ABp, AB, gam, gA, gB, g.ps.b_dummy);
+        der_dir<J, 1>(A, ABp, AB, gam, gA, gB, g.ps.b_dummy);
+        der_dir<J, 2>(A, ABp, AB, gam, gA, gB, g.ps.b_dummy);
     }
-    template <int... Ks>
-    __device__ __forceinline__ static void der_all(const Acc& acc, const ABt& ABp, const double* AB,
+    template <int... Js>
+    __device__ __forceinline__ static void der_all(const Acc& A, const ABt& ABp, const double* AB,
                                                    const TmplArgs& g, long aoA, long aoB, long aoC, double (&gA)[3],
-                                                   double (&gB)[3], std::integer_sequence<int, Ks...>) {
-        (der_one<Ks>(acc, ABp, AB, g, aoA, aoB, aoC, gA, gB), ...);
+                                                   double (&gB)[3], std::integer_sequence<int, Js...>) {
+        (der_one<Js>(A, ABp, AB, g, aoA, aoB, aoC, gA, gB), ...);
     }
 };
 
 template <class CL>
 __device__ __forceinline__ void rys_thread_body(const TmplArgs& g, long task, double* sgrad) {
-    constexpr int NR = CL::NR, NM = CL::NM, MM = CL::MM, LB = CL::LB;
+    constexpr int NR = CL::NR, NM = CL::NM, LB = CL::LB;
     const long tp = g.naux_grid > 0 ? task / g.naux_grid : task;
     const long ta = g.naux_grid > 0 ? task - tp * g.naux_grid : task;
     const int pair = g.task_pair[tp];
     const int C = g.task_aux[ta];
     const int shA = g.ps.shA[pair];
     const int shB = g.ps.b_dummy ? -1 : g.ps.shB[pair];
+    if (CL::MODE == 3 && g.ps.b_dummy) return;  // no B centre
     double A[3], AB[3], Cc[3];
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
@@ -317,12 +391,7 @@ __device__ __forceinline__ void rys_thread_body(const TmplArgs& g, long task, do
     const int nc = g.ax.nprim[C];
 
     typename CL::Acc acc;
-#pragma unroll
-    for (int w = 0; w < CL::NW; ++w)
-#pragma unroll
-        for (int e = 0; e < CL::NE; ++e)
-#pragma unroll
-            for (int f = 0; f < CL::NL; ++f) acc[w][e][f] = 0.0;
+    CL::zero(acc);
 
     for (int iab = 0; iab < nab; ++iab) {
         const double p = g.ps.eta[p0 + iab];
@@ -353,11 +422,13 @@ __device__ __forceinline__ void rys_thread_body(const TmplArgs& g, long task, do
                 const double B0 = x * 0.5 * inv;
                 const double B1 = (1.0 - x) * h_p + B0;
                 const double B1p = (1.0 - x) * h_q + B0;
-                typename CL::Gt Gx, Gy, Gz;
-                build_G_t<NM, MM>(Gx, pref * wr[u], PA[0] + qi * x * CP[0], -pi * x * CP[0], B0, B1, B1p);
-                build_G_t<NM, MM>(Gy, 1.0, PA[1] + qi * x * CP[1], -pi * x * CP[1], B0, B1, B1p);
-                build_G_t<NM, MM>(Gz, 1.0, PA[2] + qi * x * CP[2], -pi * x * CP[2], B0, B1, B1p);
-                CL::acc_all(acc, Gx, Gy, Gz, a2, b2, std::make_integer_sequence<int, CL::NE * CL::NL>{});
+                typename CL::GtX Gx;
+                typename CL::GtY Gy;
+                typename CL::GtZ Gz;
+                build_G_t<NM, CL::MDX>(Gx, pref * wr[u], PA[0] + qi * x * CP[0], -pi * x * CP[0], B0, B1, B1p);
+                build_G_t<NM, CL::MDY>(Gy, 1.0, PA[1] + qi * x * CP[1], -pi * x * CP[1], B0, B1, B1p);
+                build_G_t<NM, CL::MDZ>(Gz, 1.0, PA[2] + qi * x * CP[2], -pi * x * CP[2], B0, B1, B1p);
+                CL::acc_all(acc, Gx, Gy, Gz, a2, b2);
             }
         }
     }
@@ -387,14 +458,16 @@ __device__ __forceinline__ void rys_thread_body(const TmplArgs& g, long task, do
 #pragma unroll
         for (int d = 0; d < 3; ++d) {
             const double vA = fac * gA[d], vB = fac * gB[d];
-            atomicAdd(G + 3 * atA + d, vA);
-            if (atB >= 0) atomicAdd(G + 3 * atB + d, vB);
+            if (CL::MODE != 3) atomicAdd(G + 3 * atA + d, vA);
+            if (CL::MODE != 2 && atB >= 0) atomicAdd(G + 3 * atB + d, vB);
             atomicAdd(G + 3 * atC + d, -(vA + vB));
         }
     }
 }
 
-template <int LA, int LB, int LC, int FS, bool DERIV>
+// grid.y enumerates (pass, component subset): SPLIT derivative classes run the
+// centre-A pass on y < FS and the centre-B pass on FS <= y < 2 FS.
+template <int LA, int LB, int LC, int FS, bool DERIV, bool SPLIT>
 __global__ void __launch_bounds__(128) k_rys_thread(TmplArgs g) {
     extern __shared__ double sgrad[];
     const int ng = (DERIV && g.smem_grad) ? g.natm * 3 : 0;
@@ -402,29 +475,24 @@ __global__ void __launch_bounds__(128) k_rys_thread(TmplArgs g) {
         for (int i = threadIdx.x; i < ng; i += blockDim.x) sgrad[i] = 0.0;
         __syncthreads();
     }
+    constexpr int M0 = !DERIV ? 0 : (SPLIT ? 2 : 1);
     const long task = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (task < g.ntask) {
         switch (blockIdx.y) {
-#define DFB_FSI(I)                                                                                            \
-    case I:                                                                                                   \
-        if constexpr (I < FS) rys_thread_body<Cls<LA, LB, LC, FS, (I < FS ? I : 0), DERIV>>(g, task, sgrad); \
+#define DFB_FSI(I)                                                                                              \
+    case I:                                                                                                     \
+        if constexpr (I < FS)                                                                                   \
+            rys_thread_body<Cls<LA, LB, LC, FS, (I < FS ? I : 0), M0>>(g, task, sgrad);                         \
+        else if constexpr (SPLIT && I < 2 * FS)                                                                 \
+            rys_thread_body<Cls<LA, LB, LC, FS, (I >= FS && I < 2 * FS ? I - FS : 0), 3>>(g, task, sgrad);      \
         break;
-            DFB_FSI(0)
-            DFB_FSI(1)
-            DFB_FSI(2)
-            DFB_FSI(3)
-            DFB_FSI(4)
-            DFB_FSI(5)
-            DFB_FSI(6)
-            DFB_FSI(7)
-            DFB_FSI(8)
-            DFB_FSI(9)
-            DFB_FSI(10)
-            DFB_FSI(11)
-            DFB_FSI(12)
-            DFB_FSI(13)
-            DFB_FSI(14)
-            DFB_FSI(15)
+            DFB_FSI(0) DFB_FSI(1) DFB_FSI(2) DFB_FSI(3) DFB_FSI(4) DFB_FSI(5) DFB_FSI(6) DFB_FSI(7)
+            DFB_FSI(8) DFB_FSI(9) DFB_FSI(10) DFB_FSI(11) DFB_FSI(12) DFB_FSI(13) DFB_FSI(14) DFB_FSI(15)
+            DFB_FSI(16) DFB_FSI(17) DFB_FSI(18) DFB_FSI(19) DFB_FSI(20) DFB_FSI(21) DFB_FSI(22) DFB_FSI(23)
+            DFB_FSI(24) DFB_FSI(25) DFB_FSI(26) DFB_FSI(27) DFB_FSI(28) DFB_FSI(29) DFB_FSI(30) DFB_FSI(31)
+            DFB_FSI(32) DFB_FSI(33) DFB_FSI(34) DFB_FSI(35) DFB_FSI(36) DFB_FSI(37) DFB_FSI(38) DFB_FSI(39)
+            DFB_FSI(40) DFB_FSI(41) DFB_FSI(42) DFB_FSI(43) DFB_FSI(44) DFB_FSI(45) DFB_FSI(46) DFB_FSI(47)
+            DFB_FSI(48) DFB_FSI(49) DFB_FSI(50) DFB_FSI(51) DFB_FSI(52) DFB_FSI(53) DFB_FSI(54) DFB_FSI(55)
 #undef DFB_FSI
             default:
                 break;

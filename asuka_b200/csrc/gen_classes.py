@@ -17,9 +17,9 @@ import os
 HERE = os.path.dirname(os.path.abspath(__file__))
 LA_MAX = 3   # AO shells up to f
 LC_MAX = 6   # aux shells up to i
-FS_MAX = 16
-ACC_BUDGET = {False: 36, True: 60}   # doubles of accumulators per thread
-G_BUDGET = 48                          # doubles of the three 2D recurrence tables
+FS_MAX = 28
+ACC_BUDGET = {False: 40, True: 66}   # doubles of accumulators per thread
+G_BUDGET = 48                          # doubles of the three 2D recurrence tables (column-limited)
 
 
 def ncart(l):
@@ -30,20 +30,48 @@ def ncb(L):
     return L * (L + 1) * (L + 2) // 6
 
 
+def comps(l):
+    return [(x, y, l - x - y) for x in range(l, -1, -1) for y in range(l - x, -1, -1)]
+
+
+def g_cost(nm, lc, nfs):
+    """Largest column-limited recurrence-table size over the subsets of a split."""
+    cs = comps(lc)
+    worst = 0
+    for f0 in range(0, len(cs), nfs):
+        sub = cs[f0:f0 + nfs]
+        worst = max(worst, (nm + 1) * sum(max(c[d] for c in sub) + 1 for d in range(3)))
+    return worst
+
+
+def nrange(lo, hi):
+    return ncb(hi + 1) - ncb(lo) if hi >= lo else 0
+
+
+def acc_per_f(la, lb, mode):
+    """Accumulator doubles per aux component for the kernel modes of dfb_rys_tmpl.cuh."""
+    if mode == 0:
+        return nrange(la, la + lb)
+    if mode == 1:
+        return 3 * nrange(max(la - 1, 0), la + lb + 1)
+    if mode == 2:
+        return (nrange(la - 1, la + lb - 1) if la > 0 else 0) + nrange(la + 1, la + lb + 1)
+    return nrange(la, la + lb - 1) + nrange(la, la + lb + 1)
+
+
 def plan(la, lb, lc, deriv):
+    """(FS, SPLIT) for a class, or None when it stays on the generic warp kernel."""
     nm = la + lb + (1 if deriv else 0)
-    lmin = (la - 1 if la > 0 else 0) if deriv else la
-    ne = ncb(nm + 1) - ncb(lmin)
     nf = ncart(lc)
-    nw = 3 if deriv else 1
-    if 3 * (nm + 1) * (lc + 1) > G_BUDGET:
-        return None
-    for fs in range(1, min(nf, FS_MAX) + 1):
-        nfs = -(-nf // fs)
-        if -(-nf // nfs) != fs:
-            continue  # keep the split exact (no empty subsets)
-        if nw * ne * nfs <= ACC_BUDGET[deriv]:
-            return fs
+    modes = [(1, False), (None, True)] if deriv else [(0, False)]
+    for mode, split in modes:
+        per_f = max(acc_per_f(la, lb, 2), acc_per_f(la, lb, 3)) if split else acc_per_f(la, lb, mode)
+        for fs in range(1, min(nf, FS_MAX) + 1):
+            nfs = -(-nf // fs)
+            if -(-nf // nfs) != fs:
+                continue  # keep the split exact (no empty subsets)
+            if per_f * nfs <= ACC_BUDGET[deriv] and g_cost(nm, lc, nfs) <= G_BUDGET:
+                return fs, split
     return None
 
 
@@ -57,9 +85,9 @@ def main() -> None:
             cls = []
             for lb in range(la + 1):
                 for lc in range(LC_MAX + 1):
-                    fs = plan(la, lb, lc, deriv)
-                    if fs is not None:
-                        cls.append((la, lb, lc, fs))
+                    pl = plan(la, lb, lc, deriv)
+                    if pl is not None:
+                        cls.append((la, lb, lc, *pl))
             if not cls:
                 continue
             name = f"dfb_cls_{'d' if deriv else 'i'}{la}"
@@ -72,10 +100,10 @@ def main() -> None:
                 f"int {name}_launch(int la, int lb, int lc, const TmplArgs& g, long nblk, size_t smem, cudaStream_t st) {{",
                 "    (void)la;",
             ]
-            for (a, b, c, fs) in cls:
-                kern = f"k_rys_thread<{a}, {b}, {c}, {fs}, {'true' if deriv else 'false'}>"
+            for (a, b, c, fs, split) in cls:
+                kern = f"k_rys_thread<{a}, {b}, {c}, {fs}, {'true' if deriv else 'false'}, {'true' if split else 'false'}>"
                 lines.append(f"    if (lb == {b} && lc == {c}) {{")
-                lines.append(f"        {kern}<<<dim3((unsigned)nblk, {fs}), 128, smem, st>>>(g);")
+                lines.append(f"        {kern}<<<dim3((unsigned)nblk, {fs * (2 if split else 1)}), 128, smem, st>>>(g);")
                 lines.append("        return 1;")
                 lines.append("    }")
             lines += ["    return 0;", "}", "}  // namespace dfb", ""]
