@@ -140,23 +140,17 @@ def _dist_setup(n_gpus: int):
 
 
 def _reduce_max(x: float, world: int) -> float:
-    if world == 1:
-        return x
-    import torch
-    import torch.distributed as dist
+    from asuka_b200.dist import max_over_ranks
 
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
+    return max_over_ranks(x)
 
 
 def _barrier(world: int) -> None:
     import torch
 
-    if world > 1:
-        import torch.distributed as dist
+    from asuka_b200.dist import barrier
 
-        dist.barrier()
+    barrier()
     torch.cuda.synchronize()
 
 

@@ -1,0 +1,61 @@
+"""Host-side logic: basis packing, shell pairs, geometries, one-electron integrals, packing, DIIS."""
+
+import numpy as np
+
+from _util import bases_of, golden
+from asuka_b200 import basis as bm
+from asuka_b200 import geometry as geo
+from asuka_b200.int1e import build_S_T
+
+
+def test_basis_sizes_match_reference_fixtures():
+    for name, nao, naux in (("n2_masvp", 38, 170), ("h2o_masvp", 29, 115), ("h2o_matzvp", 52, 228)):
+        g = golden(name)
+        ao, aux, sp = bases_of(g)
+        assert (ao.nao, aux.nao) == (nao, naux)
+        assert g["S"].shape == (nao, nao)
+
+
+def test_shell_pairs_are_l_ordered_and_complete():
+    ao = bm.pack_basis(list(geo.water("ma-tzvp").atoms_bohr), "ma-tzvp", "ao")
+    sp = bm.build_shell_pairs_l_order(ao)
+    n = ao.nshell
+    assert sp.nsp == n * (n + 1) // 2
+    assert np.all(ao.shell_l[sp.sp_A] >= ao.shell_l[sp.sp_B])
+    pairs = {(min(a, b), max(a, b)) for a, b in zip(sp.sp_A, sp.sp_B)}
+    assert len(pairs) == sp.nsp
+    assert sp.sp_pair_start[-1] == np.sum(ao.shell_nprim[sp.sp_A] * ao.shell_nprim[sp.sp_B])
+
+
+def test_workload_sizes():
+    mol = geo.water_cluster(8, 0, "ma-tzvp")
+    ao = bm.pack_basis(list(mol.atoms_bohr), "ma-tzvp", "ao")
+    aux = bm.pack_basis(list(mol.atoms_bohr), "ma-tzvp", "aux")
+    assert (ao.nao, aux.nao) == (416, 1824)
+    R = mol.coords_bohr[0::3] / geo.ANGSTROM_TO_BOHR
+    d = np.linalg.norm(R[:, None] - R[None], axis=-1) + np.eye(8) * 10
+    assert d.min() >= 2.7
+    dec = geo.decane(0, "ma-svp")
+    assert dec.natm == 32 and dec.nelectron == 82
+
+
+def test_overlap_matches_reference():
+    for name in ("n2_masvp", "h2o_matzvp"):
+        g = golden(name)
+        ao, aux, sp = bases_of(g)
+        S, T = build_S_T(ao)
+        assert np.abs(S - g["S"]).max() < 1e-13
+
+
+def test_nuclear_repulsion_gradient_matches_finite_difference():
+    mol = geo.water("ma-svp")
+    g = mol.energy_nuc_grad()
+    h = 1e-5
+    for a in range(mol.natm):
+        for c in range(3):
+            R = mol.coords_bohr.copy()
+            R[a, c] += h
+            ep = mol.with_coords(R).energy_nuc()
+            R[a, c] -= 2 * h
+            em = mol.with_coords(R).energy_nuc()
+            assert abs((ep - em) / (2 * h) - g[a, c]) < 1e-7
