@@ -41,6 +41,9 @@ _SIGS = {
                                                           ctypes.c_int, _d, ctypes.c_long, _d]),
     "dfb_rys_scratch_doubles": (ctypes.c_long, [ctypes.c_int] * 3 + [ctypes.c_long, ctypes.c_int]),
     "dfb_fp64_fma_probe": (ctypes.c_int, [_d, ctypes.c_int, ctypes.c_int, ctypes.c_int, _d]),
+    "dfb_rys_int_noalloc": (ctypes.c_int, [ctypes.c_int] * 3 + [ctypes.POINTER(PairSide), ctypes.POINTER(AuxSide), _d,
+                                                                _d, ctypes.c_long, ctypes.c_long, ctypes.c_int, _d,
+                                                                ctypes.c_long, ctypes.c_long, ctypes.c_long, _d]),
 }
 
 _LIB = None

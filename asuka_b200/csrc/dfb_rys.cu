@@ -464,7 +464,8 @@ template <int KB, bool DERIV>
 static int launch_rys(const ClassInfo& ci, const dfb_pair_side_t* ps, const dfb_aux_side_t* ax,
                       const int* task_pair, const int* task_aux, long ntask, long naux_grid, int mode, double* out,
                       long sP, long sM, long sN, const double* bar, long sbP, long sbM, long sbN, double* grad, int natm,
-                      double* scratch, long scratch_doubles, cudaStream_t st, int query_only, long* need) {
+                      double* scratch, long scratch_doubles, cudaStream_t st, int query_only, long* need,
+                      int fit_grid_to_scratch = 0) {
     const int dev = current_device();
     const int smem_grad = (DERIV && natm * 3 <= 4096) ? 1 : 0;
     const size_t smem =
@@ -494,6 +495,15 @@ static int launch_rys(const ClassInfo& ci, const dfb_pair_side_t* ps, const dfb_
     if (blocks > blocks_needed) blocks = blocks_needed;
     if (blocks < 1) blocks = 1;
     const long slot = (DERIV ? 3L : 1L) * ci.nef;
+    if (fit_grid_to_scratch) {
+        // fixed scratch: shrink the persistent grid until its warp slots fit
+        const long fit = scratch_doubles / (DFB_WARPS_PER_BLOCK * slot);
+        if (fit < 1)
+            return set_error(DFB_ERR_UNSUPPORTED,
+                             "class (%d,%d,%d) needs %ld scratch doubles per block, the fixed scratch holds %ld",
+                             ci.la, ci.lb, ci.lc, (long)DFB_WARPS_PER_BLOCK * slot, scratch_doubles);
+        if (blocks > fit) blocks = fit;
+    }
     const long required = blocks * DFB_WARPS_PER_BLOCK * slot;
     if (query_only) {
         *need = required;
@@ -514,7 +524,8 @@ template <bool DERIV>
 static int dispatch_rys(int la, int lb, int lc, const dfb_pair_side_t* ps, const dfb_aux_side_t* ax,
                         const int* task_pair, const int* task_aux, long ntask, long naux_grid, int mode, double* out,
                         long sP, long sM, long sN, const double* bar, long sbP, long sbM, long sbN, double* grad, int natm,
-                        double* scratch, long scratch_doubles, cudaStream_t st, int query_only, long* need) {
+                        double* scratch, long scratch_doubles, cudaStream_t st, int query_only, long* need,
+                        int fit_grid_to_scratch = 0) {
     if (la < 0 || lb < 0 || lc < 0 || la > DFB_LMAX || lb > DFB_LMAX || lc > DFB_LMAX)
         return set_error(DFB_ERR_UNSUPPORTED, "angular momentum out of range (la=%d lb=%d lc=%d, max %d)", la, lb, lc,
                          DFB_LMAX);
@@ -573,7 +584,8 @@ static int dispatch_rys(int la, int lb, int lc, const dfb_pair_side_t* ps, const
 #define DFB_CASE(K)                                                                                              \
     if (kb <= K)                                                                                                 \
         return launch_rys<K, DERIV>(ci, ps, ax, task_pair, task_aux, ntask, naux_grid, mode, out, sP, sM, sN, bar, sbP, sbM, \
-                                    sbN, grad, natm, scratch, scratch_doubles, st, query_only, need);
+                                    sbN, grad, natm, scratch, scratch_doubles, st, query_only, need,      \
+                                    fit_grid_to_scratch);
     DFB_CASE(1)
     DFB_CASE(2)
     DFB_CASE(4)
@@ -581,7 +593,7 @@ static int dispatch_rys(int la, int lb, int lc, const dfb_pair_side_t* ps, const
     DFB_CASE(16)
 #undef DFB_CASE
     return launch_rys<16, DERIV>(ci, ps, ax, task_pair, task_aux, ntask, naux_grid, mode, out, sP, sM, sN, bar, sbP, sbM, sbN,
-                                 grad, natm, scratch, scratch_doubles, st, query_only, need);
+                                 grad, natm, scratch, scratch_doubles, st, query_only, need, fit_grid_to_scratch);
 }
 
 }  // namespace dfb
@@ -673,4 +685,51 @@ extern "C" long dfb_rys_scratch_doubles(int la, int lb, int lc, long ntask, int 
         rc = dispatch_rys<false>(la, lb, lc, &ps, &ax, nullptr, nullptr, ntask, 0, 0, nullptr, 0, 0, 0, nullptr, 0, 0,
                                  0, nullptr, 1, nullptr, 0, 0, 1, &need);
     return rc == DFB_OK ? need : (long)rc;
+}
+
+// ---------------------------------------------------------------------------
+// Allocation-free variant of dfb_rys_int.
+//
+// Callers that cannot allocate device memory at the point where they need
+// integrals -- a host framework that hands this library only its input and
+// output buffers, code running under an external allocator that forbids new
+// device allocations, or a plugin that must not touch the caller's memory
+// pool -- cannot provide the scratch buffer dfb_rys_int requires for classes
+// that run on the generic warp kernel.  This entry point uses a fixed scratch
+// array that lives in the library's own device image instead.
+//
+// The array below is DFB_NOALLOC_SCRATCH_DOUBLES doubles (8 MiB) and every GPU
+// that loads the library keeps it until the process exits.  Host code only
+// sees a host-side stand-in for it, so its device address is looked up with
+// cudaGetSymbolAddress on the first call on each device (with that device
+// current) and cached; make that first call before any stream capture.  All
+// calls share the array: each task overwrites the part it reads, so nothing
+// needs clearing between calls, but calls that overlap on the GPU (different
+// streams, or concurrent host threads) race on it and must be serialised by
+// the caller.  When a class needs more than the array holds per block of the
+// persistent grid, the grid is shrunk to fit; when not even one block fits, the
+// call fails with DFB_ERR_UNSUPPORTED and a message naming the sizes.
+// ---------------------------------------------------------------------------
+
+#define DFB_NOALLOC_SCRATCH_DOUBLES (1L << 20)
+static __device__ __align__(256) double g_noalloc_scratch[DFB_NOALLOC_SCRATCH_DOUBLES];
+static double* g_noalloc_ptr[64];
+
+extern "C" int dfb_rys_int_noalloc(int la, int lb, int lc, const dfb_pair_side_t* ps, const dfb_aux_side_t* aux,
+                                   const int* task_pair, const int* task_aux, long ntask, long naux_grid, int mode,
+                                   double* out, long sP, long sM, long sN, void* stream) {
+    clear_error();
+    if (!ps || !aux || (ntask > 0 && (!task_pair || !task_aux || !out)) || (mode != 0 && mode != 1))
+        return set_error(DFB_ERR_INVALID, "invalid arguments to dfb_rys_int_noalloc");
+    const int dev = current_device();
+    if (dev < 0 || dev >= 64) return set_error(DFB_ERR_INVALID, "device index %d out of range", dev);
+    if (g_noalloc_ptr[dev] == nullptr) {
+        void* p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess) return set_cuda_error("cudaGetSymbolAddress(g_noalloc_scratch)", e);
+        g_noalloc_ptr[dev] = static_cast<double*>(p);
+    }
+    return dispatch_rys<false>(la, lb, lc, ps, aux, task_pair, task_aux, ntask, naux_grid, mode, out, sP, sM, sN,
+                               nullptr, 0, 0, 0, nullptr, 0, g_noalloc_ptr[dev], DFB_NOALLOC_SCRATCH_DOUBLES,
+                               (cudaStream_t)stream, 0, nullptr, 1);
 }

@@ -114,6 +114,23 @@ int dfb_rys_deriv(int la, int lb, int lc, const dfb_pair_side_t *ps, const dfb_a
  */
 int dfb_fp64_fma_probe(double *out, int blocks, int threads, int iters, void *stream);
 
+/*
+ * Allocation-free variant of dfb_rys_int for callers that cannot allocate
+ * device memory (frameworks that hand over only input/output buffers, code
+ * under an allocator that forbids new device allocations).  No counterpart in
+ * the reference.  Same arguments and output as dfb_rys_int without the
+ * scratch buffer: the generic warp kernel uses a fixed 8 MiB scratch array in
+ * the library's device image (held by every GPU that loads the library), the
+ * persistent grid is shrunk to fit it, and classes that need more than it holds
+ * per block fail with DFB_ERR_UNSUPPORTED.  The first call on a device looks up
+ * the array's address and should come before any stream capture; calls share
+ * the array, so calls that overlap on the GPU race.  dfb_rys_table_init must
+ * have run on the device.
+ */
+int dfb_rys_int_noalloc(int la, int lb, int lc, const dfb_pair_side_t *ps, const dfb_aux_side_t *aux,
+                        const int *task_pair, const int *task_aux, long ntask, long naux_grid, int mode, double *out,
+                        long sP, long sM, long sN, void *stream);
+
 /* Scratch doubles dfb_rys_int / dfb_rys_deriv need for this class and task count. */
 long dfb_rys_scratch_doubles(int la, int lb, int lc, long ntask, int deriv);
 
