@@ -31,7 +31,7 @@ _SIGS = {
     "dfb_rys_table_init": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_long, ctypes.c_void_p,
                                           ctypes.c_void_p, ctypes.c_long, ctypes.c_int, ctypes.c_int, ctypes.c_int,
                                           ctypes.c_double]),
-    "dfb_pair_tables": (ctypes.c_int, [_d] * 9 + [ctypes.c_long, ctypes.c_int] + [_d] * 7 + [_d]),
+    "dfb_pair_tables": (ctypes.c_int, [_d] * 10 + [ctypes.c_long, ctypes.c_int] + [_d] * 7 + [_d]),
     "dfb_rys_int": (ctypes.c_int, [ctypes.c_int] * 3 + [ctypes.POINTER(PairSide), ctypes.POINTER(AuxSide), _d, _d,
                                                         ctypes.c_long, ctypes.c_long, ctypes.c_int, _d, ctypes.c_long,
                                                         ctypes.c_long, ctypes.c_long, _d, ctypes.c_long, _d]),

@@ -30,6 +30,14 @@ def needs_build() -> bool:
     return any(os.path.getmtime(p) > t for p in deps if os.path.exists(p))
 
 
+def _flags_changed(objdir: str, flags: list[str]) -> bool:
+    p = os.path.join(objdir, "flags.txt")
+    if not os.path.exists(p):
+        return True
+    with open(p) as f:
+        return f.read() != " ".join(flags)
+
+
 def build(force: bool = False, verbose: bool = False, jobs: int | None = None) -> str:
     """Compile every csrc/*.cu to an object in parallel (they are independent), then link."""
     if not force and not needs_build():
@@ -41,9 +49,15 @@ def build(force: bool = False, verbose: bool = False, jobs: int | None = None) -
     procs = []
     objs = []
     jobs = jobs or max(1, os.cpu_count() or 1)
+    headers = glob.glob(os.path.join(CSRC, "*.cuh")) + glob.glob(os.path.join(CSRC, "*.h"))
+    headers.append(os.path.join(HERE, "..", "include", "dfb.h"))
+    t_hdr = max(os.path.getmtime(h) for h in headers if os.path.exists(h))
     for src in sources():
         obj = os.path.join(objdir, os.path.basename(src)[:-3] + ".o")
         objs.append(obj)
+        if (not force and os.path.exists(obj) and os.path.getmtime(obj) >= os.path.getmtime(src)
+                and os.path.getmtime(obj) >= t_hdr and not _flags_changed(objdir, compile_flags)):
+            continue
         cmd = [nvcc, *compile_flags, "-c", src, "-o", obj]
         if verbose:
             print(" ".join(cmd), flush=True)
@@ -55,6 +69,8 @@ def build(force: bool = False, verbose: bool = False, jobs: int | None = None) -
             raise RuntimeError(f"nvcc failed: {p.args}")
     subprocess.run([nvcc, "-gencode", "arch=compute_100a,code=sm_100a", "--shared", "-o", OUT + ".tmp", *objs],
                    check=True, cwd=CSRC)
+    with open(os.path.join(objdir, "flags.txt"), "w") as f:
+        f.write(" ".join(compile_flags))
     os.replace(OUT + ".tmp", OUT)
     return OUT
 

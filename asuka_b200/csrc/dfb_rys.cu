@@ -403,13 +403,14 @@ __global__ void k_pair_tables(const double* __restrict__ cxyz, const int* __rest
                               const int* __restrict__ nprim_sh, const double* __restrict__ pexp,
                               const double* __restrict__ pcoef, const int* __restrict__ sp_A,
                               const int* __restrict__ sp_B, const int* __restrict__ sp_pstart,
-                              const int* __restrict__ pp_sp, long npp, int b_dummy, double* eta, double* Px,
+                              const int* __restrict__ pp_sp, const int* __restrict__ pp_local, long npp, int b_dummy,
+                              double* eta, double* Px,
                               double* Py, double* Pz, double* cK, double* ea, double* eb) {
     const long i = (long)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= npp) return;
     const int sp = pp_sp[i];
     const int A = sp_A[sp];
-    const int local = (int)(i - sp_pstart[sp]);
+    const int local = pp_local ? pp_local[i] : (int)(i - sp_pstart[sp]);
     if (b_dummy) {
         const double a = pexp[spstart_sh[A] + local];
         eta[i] = a;
@@ -633,15 +634,16 @@ extern "C" int dfb_rys_table_init(const double* coef, const int* offs, long ncoe
 
 extern "C" int dfb_pair_tables(const double* cxyz, const int* shell_pstart, const int* shell_nprim,
                                const double* pexp, const double* pcoef, const int* sp_A, const int* sp_B,
-                               const int* sp_pstart, const int* pp_sp, long npp, int b_dummy, double* eta, double* Px,
+                               const int* sp_pstart, const int* pp_sp, const int* pp_local, long npp, int b_dummy,
+                               double* eta, double* Px,
                                double* Py, double* Pz, double* cK, double* ea, double* eb, void* stream) {
     clear_error();
     if (npp < 0) return set_error(DFB_ERR_INVALID, "npp < 0");
     if (npp == 0) return DFB_OK;
     const unsigned blocks = (unsigned)((npp + 255) / 256);
     k_pair_tables<<<blocks, 256, 0, (cudaStream_t)stream>>>(cxyz, shell_pstart, shell_nprim, pexp, pcoef, sp_A, sp_B,
-                                                            sp_pstart, pp_sp, npp, b_dummy, eta, Px, Py, Pz, cK, ea,
-                                                            eb);
+                                                            sp_pstart, pp_sp, pp_local, npp, b_dummy, eta, Px, Py,
+                                                            Pz, cK, ea, eb);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return set_cuda_error("k_pair_tables launch", e);
     return DFB_OK;

@@ -35,6 +35,7 @@ from .basis import BasisCartSoA, build_shell_pairs_l_order, from_reference_like,
 
 _DATA = os.path.join(os.path.dirname(os.path.abspath(__file__)), "data")
 _TABLE_READY: set[int] = set()
+PRIM_SCREEN = 1e-20  # primitive-pair magnitude bound below which a pair is skipped (0 = evaluate all)
 NROOTS_SLOTS = 11  # DFB_NROOTS_MAX + 1
 
 
@@ -84,7 +85,8 @@ def _as_soa(b) -> BasisCartSoA:
 class DFEngine:
     """Device-side state of the DF Rys integrals for one (AO, aux) basis pair."""
 
-    def __init__(self, ao_basis, aux_basis, device=None, atom_coords_bohr: np.ndarray | None = None):
+    def __init__(self, ao_basis, aux_basis, device=None, atom_coords_bohr: np.ndarray | None = None,
+                 prim_screen: float = PRIM_SCREEN):
         self.device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
         if self.device.type != "cuda":
             raise RuntimeError("DFEngine runs on CUDA devices only (no CPU fallback)")
@@ -101,13 +103,14 @@ class DFEngine:
         self.ao, self.aux = ao, aux
         self.nao, self.naux = ao.nao, aux.nao
         self.natm = int(max(ao.shell_atom.max(initial=-1), aux.shell_atom.max(initial=-1))) + 1
+        self.prim_screen = float(prim_screen)
         if ao.lmax > 8 or aux.lmax > 8:
             raise NotImplementedError("shells with l > 8 are not supported")
         dev = self.device
-        i32 = lambda a: torch.as_tensor(np.ascontiguousarray(a, dtype=np.int32), device=dev)  # noqa: E731
-        f64 = lambda a: torch.as_tensor(np.ascontiguousarray(a, dtype=np.float64), device=dev)  # noqa: E731
+        i32 = self._i32
+        f64 = self._f64
 
-        # ---- AO side: basis arrays, l-ordered shell pairs, primitive-pair tables
+        # ---- AO side: basis arrays and l-ordered shell pairs
         self.sp = build_shell_pairs_l_order(ao)
         self.ao_cxyz = f64(ao.shell_cxyz)
         self.ao_pstart = i32(ao.shell_prim_start)
@@ -118,11 +121,6 @@ class DFEngine:
         self.ao_atom = i32(ao.shell_atom)
         self.sp_A = i32(self.sp.sp_A)
         self.sp_B = i32(self.sp.sp_B)
-        self.sp_pstart = i32(self.sp.sp_pair_start[:-1])
-        self.sp_npair = i32(self.sp.sp_npair)
-        self.pp_sp = i32(np.repeat(np.arange(self.sp.nsp, dtype=np.int32), self.sp.sp_npair))
-        npp = int(self.sp.sp_pair_start[-1])
-        self.pt = torch.empty((7, max(npp, 1)), dtype=torch.float64, device=dev)
 
         # ---- aux side: basis arrays and (P, dummy) self-pair tables for the metric
         self.ax_cxyz = f64(aux.shell_cxyz)
@@ -135,36 +133,19 @@ class DFEngine:
         self.ax_self = i32(np.arange(aux.nshell, dtype=np.int32))
         self.ax_pp_sp = i32(np.repeat(np.arange(aux.nshell, dtype=np.int32), aux.shell_nprim))
         self.axpt = torch.empty((7, max(int(aux.shell_nprim.sum()), 1)), dtype=torch.float64, device=dev)
-        self._build_pair_tables()
-
-        self.ps_ao = _lib.PairSide(
-            *[_lib.ptr(t) for t in (self.sp_A, self.sp_B, self.sp_pstart, self.sp_npair, *self.pt, self.ao_cxyz,
-                                    self.ao_aostart, self.ao_atom)], 0)
         self.ps_aux = _lib.PairSide(
             *[_lib.ptr(t) for t in (self.ax_self, self.ax_self, self.ax_pstart, self.ax_nprim, *self.axpt,
                                     self.ax_cxyz, self.ax_aostart, self.ax_atom)], 1)
         self.axs = _lib.AuxSide(*[_lib.ptr(t) for t in (self.ax_cxyz, self.ax_pstart, self.ax_nprim, self.ax_exp,
                                                         self.ax_coef, self.ax_aostart, self.ax_atom)])
-
-        # ---- task classes
-        la = ao.shell_l[self.sp.sp_A]
-        lb = ao.shell_l[self.sp.sp_B]
         aux_l = aux.shell_l
         self.aux_by_l = {}
         for l in np.unique(aux_l):
             idx = np.nonzero(aux_l == l)[0]
             idx = idx[np.argsort(aux.shell_nprim[idx], kind="stable")]
             self.aux_by_l[int(l)] = i32(idx)
-        self.classes3c = []  # (la, lb, lc, pairs tensor, aux tensor)
-        for a in np.unique(la):
-            for b in np.unique(lb):
-                sel = np.nonzero((la == a) & (lb == b))[0]
-                if sel.size == 0:
-                    continue
-                pairs = i32(sel)
-                for c, auxs in self.aux_by_l.items():
-                    self.classes3c.append((int(a), int(b), int(c), pairs, auxs))
-        self.classes2c = []  # (lp, lq, P tensor, Q tensor) explicit lists, P "pair" side
+        # metric classes: unordered aux pairs oriented l(P) >= l(Q)
+        self.classes2c = []
         nsh = aux.nshell
         Pi, Qi = np.tril_indices(nsh)
         lp, lq = aux_l[Pi], aux_l[Qi]
@@ -178,25 +159,103 @@ class DFEngine:
                 if sel.size:
                     self.classes2c.append((int(a), int(c), i32(P[sel]), i32(Q[sel])))
         self._scratch = None
+        self._build_ao_pairs(ao.shell_cxyz)
+        self._build_pair_tables()
+
+    @property
+    def _i32(self):
+        return lambda a: torch.as_tensor(np.ascontiguousarray(a, dtype=np.int32), device=self.device)
+
+    @property
+    def _f64(self):
+        return lambda a: torch.as_tensor(np.ascontiguousarray(a, dtype=np.float64), device=self.device)
+
+    def _build_ao_pairs(self, shell_cxyz: np.ndarray) -> None:
+        """Primitive-pair lists (screened) and the per-class AO pair lists for a geometry.
+
+        A primitive pair is dropped when |c_a c_b| exp(-ab/(a+b) |AB|^2) (pi/(a+b))^(3/2),
+        an upper bound of its overlap-like magnitude, is below ``prim_screen`` (1e-20 by
+        default): its contribution to any integral is many orders below the FP64 rounding
+        of the integral.  Shell pairs with no primitive pair left are dropped.  The
+        reference evaluates every pair (``asuka/cueri/gpu.py:1833-1834``); ``prim_screen=0``
+        reproduces that exactly.
+        """
+        ao, sp = self.ao, self.sp
+        npr = sp.sp_npair.astype(np.int64)
+        owner = np.repeat(np.arange(sp.nsp), npr)
+        loc = (np.arange(owner.size) - np.repeat(sp.sp_pair_start[:-1].astype(np.int64), npr)).astype(np.int32)
+        A = sp.sp_A[owner]
+        B = sp.sp_B[owner]
+        nb = ao.shell_nprim[B]
+        pa = ao.shell_prim_start[A] + loc // nb
+        pb = ao.shell_prim_start[B] + loc % nb
+        if self.prim_screen > 0.0:
+            a, b = ao.prim_exp[pa], ao.prim_exp[pb]
+            R2 = ((shell_cxyz[A] - shell_cxyz[B]) ** 2).sum(1)
+            p = a + b
+            bound = np.abs(ao.prim_coef[pa] * ao.prim_coef[pb]) * np.exp(-a * b / p * R2) * (np.pi / p) ** 1.5
+            keep = bound >= self.prim_screen
+        else:
+            keep = np.ones(owner.size, dtype=bool)
+        kept_owner = owner[keep]
+        cnt = np.bincount(kept_owner, minlength=sp.nsp).astype(np.int32)
+        start = np.zeros(sp.nsp, dtype=np.int64)
+        np.cumsum(cnt[:-1], out=start[1:])
+        i32 = self._i32
+        self.sp_pstart = i32(start)
+        self.sp_npair = i32(cnt)
+        self.pp_sp = i32(kept_owner)
+        self.pp_local = i32(loc[keep])
+        self.n_prim_pairs = int(keep.sum())
+        self.n_prim_pairs_total = int(owner.size)
+        self.pt = torch.empty((7, max(self.n_prim_pairs, 1)), dtype=torch.float64, device=self.device)
+        self.ps_ao = _lib.PairSide(
+            *[_lib.ptr(t) for t in (self.sp_A, self.sp_B, self.sp_pstart, self.sp_npair, *self.pt, self.ao_cxyz,
+                                    self.ao_aostart, self.ao_atom)], 0)
+        la = ao.shell_l[sp.sp_A]
+        lb = ao.shell_l[sp.sp_B]
+        live = cnt > 0
+        # dropped shell pairs write nothing: outputs are zero-filled first when any exist
+        self.n_dropped_pairs = int((~live).sum())
+        self.classes3c = []  # (la, lb, lc, pairs tensor, aux tensor)
+        for a in np.unique(la):
+            for b in np.unique(lb):
+                sel = np.nonzero((la == a) & (lb == b) & live)[0]
+                if sel.size == 0:
+                    continue
+                pairs = i32(sel)
+                for c, auxs in self.aux_by_l.items():
+                    self.classes3c.append((int(a), int(b), int(c), pairs, auxs))
+        self._aux_blocks_n = None
 
     # ------------------------------------------------------------ helpers
     def _build_pair_tables(self) -> None:
         L = _lib.lib()
         p = _lib.ptr
-        npp = int(self.pp_sp.numel())
+        npp = self.n_prim_pairs
         rc = L.dfb_pair_tables(p(self.ao_cxyz), p(self.ao_pstart), p(self.ao_nprim), p(self.ao_exp), p(self.ao_coef),
-                               p(self.sp_A), p(self.sp_B), p(self.sp_pstart), p(self.pp_sp), npp, 0,
+                               p(self.sp_A), p(self.sp_B), p(self.sp_pstart), p(self.pp_sp), p(self.pp_local), npp, 0,
                                *[p(r) for r in self.pt], _stream())
         _lib.check(rc, "dfb_pair_tables(ao)")
         nax = int(self.ax_pp_sp.numel())
         rc = L.dfb_pair_tables(p(self.ax_cxyz), p(self.ax_pstart), p(self.ax_nprim), p(self.ax_exp), p(self.ax_coef),
-                               p(self.ax_self), p(self.ax_self), p(self.ax_pstart), p(self.ax_pp_sp), nax, 1,
+                               p(self.ax_self), p(self.ax_self), p(self.ax_pstart), p(self.ax_pp_sp), 0, nax, 1,
                                *[p(r) for r in self.axpt], _stream())
         _lib.check(rc, "dfb_pair_tables(aux)")
 
-    def set_coords(self, coords: torch.Tensor) -> None:
-        """Move the shell centres to new atom positions (device tensor (natm, 3), bohr)."""
-        coords = coords.to(device=self.device, dtype=torch.float64).reshape(-1, 3)
+    def set_coords(self, coords) -> None:
+        """Move the shell centres to new atom positions ((natm, 3), bohr).
+
+        Host coordinates (numpy or CPU tensor) also rebuild the screened primitive-pair
+        lists for the new geometry; device coordinates update the centres and pair tables
+        without a host round trip and keep the lists of the last host geometry (use them
+        for small moves, such as finite differences or the timed steps of a fixed
+        geometry).
+        """
+        if isinstance(coords, np.ndarray) or (isinstance(coords, torch.Tensor) and not coords.is_cuda):
+            c_np = np.asarray(coords, dtype=np.float64).reshape(-1, 3)
+            self._build_ao_pairs(c_np[self.ao.shell_atom])
+        coords = torch.as_tensor(coords, dtype=torch.float64).to(device=self.device).reshape(-1, 3)
         self.ao_cxyz.copy_(coords.index_select(0, self.ao_atom.long()))
         self.ax_cxyz.copy_(coords.index_select(0, self.ax_atom.long()))
         self._build_pair_tables()
@@ -250,6 +309,8 @@ class DFEngine:
         axb, _shifted, byl = blk
         nao = self.nao
         X = out if out is not None else torch.empty((p1 - p0, nao, nao), dtype=torch.float64, device=self.device)
+        if self.n_dropped_pairs:
+            X.zero_()
         scr = self._scratch_for(False)
         L = _lib.lib()
         seen = set()
@@ -290,6 +351,8 @@ class DFEngine:
         else:
             raise ValueError("layout must be 'Qmn' or 'mnQ'")
         X = out if out is not None else torch.empty(shape, dtype=torch.float64, device=self.device)
+        if self.n_dropped_pairs:
+            X.zero_()
         scr = self._scratch_for(False)
         L = _lib.lib()
         for la, lb, lc, pairs, auxs in self.classes3c:

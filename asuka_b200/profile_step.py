@@ -1,0 +1,198 @@
+"""Phase breakdown of one DF J/K + gradient step, and a driver for ncu captures.
+
+    python -m asuka_b200.profile_step [--workload w8|decane|n2] [--steps N] [--precision fp64|mixed]
+    python -m asuka_b200.profile_step --only deriv3c --steps 1     # one phase, for `ncu -k ...`
+
+Uses an orthonormal random occupied block (the step's cost does not depend on
+the density's values), so the launch list holds the step's kernels only.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+
+import numpy as np
+import torch
+
+from . import basis as bm
+from . import geometry as geo
+from .df import DFEngine, cholesky_metric
+from .grad import df_backward, df_forward
+
+WORKLOADS = {
+    "w8": lambda: geo.water_cluster(8, 0, "ma-tzvp"),
+    "decane": lambda: geo.decane(0, "ma-svp"),
+    "n2": lambda: geo.n2("ma-svp"),
+    "w1": lambda: geo.water("ma-tzvp"),
+}
+
+
+def setup(name: str):
+    mol = WORKLOADS[name]()
+    atoms = list(mol.atoms_bohr)
+    ao = bm.pack_basis(atoms, mol.basis, "ao")
+    aux = bm.pack_basis(atoms, mol.basis, "aux")
+    eng = DFEngine(ao, aux)
+    rng = np.random.default_rng(0)
+    nocc = mol.nelectron // 2
+    Cw = torch.as_tensor(np.linalg.qr(rng.standard_normal((ao.nao, nocc)))[0] * np.sqrt(2.0), device="cuda")
+    R = torch.as_tensor(mol.coords_bohr, device="cuda")
+    return mol, eng, Cw, R
+
+
+def phases(eng: DFEngine, Cw: torch.Tensor, R: torch.Tensor, precision: str, X: torch.Tensor) -> dict:
+    ev = {}
+
+    def mark(k):
+        e = torch.cuda.Event(enable_timing=True)
+        e.record()
+        ev[k] = e
+
+    mark("start")
+    eng.set_coords(R)
+    mark("pair_tables")
+    V = eng.metric()
+    mark("metric")
+    L = cholesky_metric(V)
+    mark("cholesky")
+    eng.int3c("Qmn", out=X)
+    mark("int3c")
+    # contractions (same algebra as grad.df_forward/df_backward)
+    E, J, K, saved = df_forward_from_X(eng, Cw, precision, X, L, mark)
+    mark("jk_K")
+    G3, G2 = adjoints(eng, Cw, saved)
+    mark("adjoints")
+    grad = torch.zeros((eng.natm, 3), dtype=torch.float64, device="cuda")
+    eng.deriv3c(G3, grad)
+    mark("deriv3c")
+    eng.deriv2c(G2, grad)
+    mark("deriv2c")
+    torch.cuda.synchronize()
+    keys = list(ev)
+    out = {k: ev[keys[i - 1]].elapsed_time(ev[k]) for i, k in enumerate(keys) if i > 0}
+    out["total"] = ev["start"].elapsed_time(ev[keys[-1]])
+    return out
+
+
+def df_forward_from_X(eng, Cw, precision, X, L, mark=lambda k: None):
+    from . import mixed as _mixed
+
+    nao, naux = eng.nao, eng.naux
+    nocc = Cw.shape[1]
+    X2 = X.view(naux, nao * nao)
+    D = Cw @ Cw.T
+    rho = X2 @ D.reshape(-1)
+    d = torch.cholesky_solve(rho.view(-1, 1), L).view(-1)
+    J = (d @ X2).view(nao, nao)
+    mark("jk_rho_J")
+    mm = (lambda A, B: A @ B) if precision == "fp64" else _mixed.matmul
+    Y = mm(X.view(naux * nao, nao), Cw).view(naux, nao * nocc)
+    mark("jk_Y")
+    W = torch.linalg.solve_triangular(L, Y, upper=False)
+    mark("jk_W_trsm")
+    W2 = W.view(naux, nao, nocc).permute(1, 0, 2).reshape(nao, naux * nocc)
+    K = mm(W2, W2.T.contiguous())
+    E = 0.5 * torch.dot(rho, d) - 0.25 * torch.sum(D * K)
+    return E, J, K, dict(X=X, L=L, d=d, W=W, D=D)
+
+
+def adjoints(eng, Cw, saved):
+    nao, naux = eng.nao, eng.naux
+    nocc = Cw.shape[1]
+    X, L, d, W, D = saved["X"], saved["L"], saved["d"], saved["W"], saved["D"]
+    M = torch.matmul(Cw.T, W.view(naux, nao, nocc))
+    M = 0.5 * (M + M.transpose(1, 2))
+    Z = torch.linalg.solve_triangular(L.T, M.reshape(naux, nocc * nocc), upper=True)
+    T = torch.matmul(Z.view(naux, nocc, nocc), Cw.T)
+    torch.matmul(Cw, T, out=X)
+    X.mul_(-0.5).add_(d.view(naux, 1, 1) * D.view(1, nao, nao))
+    G2 = -0.5 * torch.outer(d, d) + 0.25 * (Z @ Z.T)
+    return X, G2
+
+
+def class_times(eng, mol, top: int = 20) -> dict:
+    """Per-class device time of the 3c integrals and the 3c derivative contraction."""
+    import ctypes
+    import os
+    import sys
+
+    from . import _lib
+
+    sys.path.insert(0, os.path.join(os.path.dirname(os.path.abspath(__file__)), "csrc"))
+    import gen_classes
+
+    nao = eng.nao
+    X = torch.empty((eng.naux, nao, nao), dtype=torch.float64, device="cuda")
+    X.fill_(1e-3)
+    g = torch.zeros((eng.natm, 3), dtype=torch.float64, device="cuda")
+    st = int(torch.cuda.current_stream().cuda_stream)
+    L = _lib.lib()
+    out = {}
+    for deriv in (False, True):
+        scr = eng._scratch_for(deriv)
+        res = []
+        for la, lb, lc, pairs, auxs in eng.classes3c:
+            args = [la, lb, lc, ctypes.byref(eng.ps_ao), ctypes.byref(eng.axs), _lib.ptr(pairs), _lib.ptr(auxs),
+                    pairs.numel() * auxs.numel(), auxs.numel(), 0, _lib.ptr(X), nao * nao, nao, 1]
+            fn = L.dfb_rys_deriv if deriv else L.dfb_rys_int
+            if deriv:
+                args += [_lib.ptr(g), eng.natm]
+            args += [_lib.ptr(scr), scr.numel(), st]
+            fn(*args)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            for _ in range(3):
+                _lib.check(fn(*args), "class timing")
+            e1.record()
+            torch.cuda.synchronize()
+            plan = gen_classes.plan(la, lb, lc, deriv) if la <= gen_classes.LA_MAX and lc <= gen_classes.LC_MAX else None
+            res.append((e0.elapsed_time(e1) / 3, f"({la},{lb},{lc})", pairs.numel() * auxs.numel(),
+                        "warp" if plan is None else f"thread FS={plan[0]}{' split' if plan[1] else ''}"))
+        res.sort(reverse=True)
+        key = "deriv3c" if deriv else "int3c"
+        out[key] = {"total_ms": round(sum(r[0] for r in res), 3),
+                    "warp_ms": round(sum(r[0] for r in res if r[3] == "warp"), 3),
+                    "top": [[round(r[0], 3), r[1], r[2], r[3]] for r in res[:top]]}
+    return out
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--workload", default="w8", choices=sorted(WORKLOADS))
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--only", default=None, choices=[None, "int3c", "deriv3c", "metric", "deriv2c", "step"])
+    ap.add_argument("--classes", action="store_true", help="time every angular class of int3c and deriv3c")
+    args = ap.parse_args()
+    mol, eng, Cw, R = setup(args.workload)
+    if args.classes:
+        print(json.dumps(class_times(eng, mol)))
+        return
+    X = torch.empty((eng.naux, eng.nao, eng.nao), dtype=torch.float64, device="cuda")
+    if args.only in ("int3c", "deriv3c", "metric", "deriv2c"):
+        g = torch.zeros((eng.natm, 3), dtype=torch.float64, device="cuda")
+        bar2 = torch.ones((eng.naux, eng.naux), dtype=torch.float64, device="cuda")
+        if args.only == "deriv3c":
+            X.fill_(1e-3)
+        for _ in range(args.steps):
+            if args.only == "int3c":
+                eng.int3c("Qmn", out=X)
+            elif args.only == "metric":
+                eng.metric()
+            elif args.only == "deriv3c":
+                eng.deriv3c(X, g)
+            else:
+                eng.deriv2c(bar2, g)
+        torch.cuda.synchronize()
+        print(json.dumps({"only": args.only, "steps": args.steps}))
+        return
+    phases(eng, Cw, R, args.precision, X)  # warm-up
+    res = [phases(eng, Cw, R, args.precision, X) for _ in range(args.steps)]
+    avg = {k: float(np.mean([r[k] for r in res])) for k in res[0]}
+    print(json.dumps({"workload": args.workload, "nao": eng.nao, "naux": eng.naux, "precision": args.precision,
+                      "ms": {k: round(v, 3) for k, v in avg.items()}}))
+
+
+if __name__ == "__main__":
+    main()

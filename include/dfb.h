@@ -68,13 +68,16 @@ int dfb_rys_table_init(const double *coef, const int *offs, long ncoef, const do
 /*
  * Primitive-pair tables: eta = a+b, P = (aA+bB)/eta, cK = ca cb exp(-ab/eta |AB|^2),
  * plus the exponents a and b.  One entry per primitive pair, pp_sp[i] = owning
- * shell pair, ordered ia*nprimB+ib inside each pair.  b_dummy=1 builds the
- * metric's (P, dummy) tables (eta=a, P=A, cK=ca, eb=0).
+ * shell pair, ordered ia*nprimB+ib inside each pair.  pp_local (optional, may be
+ * NULL) gives entry i's index ia*nprimB+ib inside its shell pair when the table
+ * holds only a subset of the pairs (screened tables); NULL means entries are
+ * dense from sp_pstart[sp].  b_dummy=1 builds the metric's (P, dummy) tables
+ * (eta=a, P=A, cK=ca, eb=0).
  * Replaces KernelBuildPairTables_ss (asuka/cueri/cuda/ext/src/cueri_cuda_kernels.cu:61-123).
  */
 int dfb_pair_tables(const double *cxyz, const int *shell_pstart, const int *shell_nprim, const double *pexp,
                     const double *pcoef, const int *sp_A, const int *sp_B, const int *sp_pstart, const int *pp_sp,
-                    long npp, int b_dummy, double *eta, double *Px, double *Py, double *Pz, double *cK, double *ea,
+                    const int *pp_local, long npp, int b_dummy, double *eta, double *Px, double *Py, double *Pz, double *cK, double *ea,
                     double *eb, void *stream);
 
 /*

@@ -136,3 +136,25 @@ def test_specialised_and_generic_kernels_agree(monkeypatch):
     assert float((X1 - X2).abs().max()) <= 1e-13 * sx
     assert float((V1 - V2).abs().max()) <= 1e-13 * float(V2.abs().max())
     assert float((g1 - g2).abs().max()) <= 1e-11 * float(g2.abs().max())
+
+
+def test_primitive_screening_changes_nothing_visible():
+    """Screened primitive pairs (bound < 1e-20) change integrals and gradients below FP64 noise."""
+    from asuka_b200.df import DFEngine
+    from asuka_b200 import geometry as geo, basis as bm
+
+    mol = geo.water_cluster(2, 1, "ma-svp")
+    atoms = list(mol.atoms_bohr)
+    ao, aux = bm.pack_basis(atoms, "ma-svp", "ao"), bm.pack_basis(atoms, "ma-svp", "aux")
+    e0 = DFEngine(ao, aux, prim_screen=0.0)
+    e1 = DFEngine(ao, aux)
+    assert e1.n_prim_pairs < e0.n_prim_pairs
+    X0, X1 = e0.int3c("Qmn"), e1.int3c("Qmn")
+    assert float((X0 - X1).abs().max()) <= 1e-14 * float(X0.abs().max())
+    bar = torch.randn_like(X0)
+    bar = bar + bar.transpose(1, 2)
+    g0 = torch.zeros((mol.natm, 3), dtype=torch.float64, device="cuda")
+    g1 = torch.zeros_like(g0)
+    e0.deriv3c(bar, g0)
+    e1.deriv3c(bar, g1)
+    assert float((g0 - g1).abs().max()) <= 1e-12 * float(g0.abs().max())

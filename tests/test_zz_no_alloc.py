@@ -43,7 +43,7 @@ def test_no_alloc_entry_matches_scratch_entry_on_two_calls(monkeypatch, generic_
         monkeypatch.setenv("DFB_DISABLE_TMPL", "1")
     g = golden("h2o_matzvp")
     ao, aux, sp = bases_of(g)
-    eng = DFEngine(ao, aux)
+    eng = DFEngine(ao, aux, prim_screen=0.0)  # every shell pair evaluated, so every output element is written
     L = _lib.lib()
     shape = (eng.naux, eng.nao, eng.nao)
     X_ref = torch.full(shape, float("nan"), dtype=torch.float64, device="cuda")
