@@ -92,9 +92,11 @@ __device__ __forceinline__ void decode_e(const ClassInfo& ci, int e, int& x, int
     decode_cart(L, e, x, y, z);
 }
 
+__constant__ int c_ncbtab[2 * DFB_LMAX + 4];  // ncart_below(L), L = 0 .. 2 LMAX + 3
+
 __device__ __forceinline__ int e_index(const ClassInfo& ci, int x, int y, int z) {
     const int L = x + y + z;
-    return ncart_below(L) - ncart_below(ci.lmin) + cart_index(x, y, L);
+    return c_ncbtab[L] - c_ncbtab[ci.lmin] + cart_index(x, y, L);
 }
 
 __constant__ double c_binomtab[DFB_LMAX + 2][DFB_LMAX + 2];
@@ -139,32 +141,27 @@ __device__ __forceinline__ void build_G(double* G, int nmax, int mmax, double g0
     }
 }
 
+// Phase 1 of the generic path: one warp per work unit (task, chunk of the
+// (e, f) elements).  Lanes evaluate 32 primitive triplets' roots at once, lanes
+// (root, direction) build the 2D recurrence tables in shared memory for one
+// triplet at a time, and every lane accumulates KB elements of the chunk.  The
+// contracted intermediate goes to the task's scratch slot: E (integrals) or
+// U | WA | WB (derivative; flushed once per AO primitive pair).  Splitting the
+// elements of a task over warps keeps the SMs busy for the heavy high-l classes,
+// which have few tasks.
 template <int KB, bool DERIV>
 __global__ void __launch_bounds__(DFB_WARPS_PER_BLOCK * 32)
-    k_rys(ClassInfo ci, dfb_pair_side_t ps, dfb_aux_side_t ax, const int* __restrict__ task_pair,
-          const int* __restrict__ task_aux, long ntask, long naux_grid, int mode, double* __restrict__ out, long sP,
-          long sM, long sN, const double* __restrict__ bar, long sbP, long sbM, long sbN, double* __restrict__ grad, int natm,
-          int smem_grad, double* __restrict__ scratch, long slot, RysTable tab) {
+    k_rys_acc(ClassInfo ci, dfb_pair_side_t ps, dfb_aux_side_t ax, const int* __restrict__ task_pair,
+              const int* __restrict__ task_aux, long t0, long nt, long naux_grid, double* __restrict__ scratch,
+              long slot, RysTable tab) {
     extern __shared__ double smem[];
     const int lane = threadIdx.x & 31;
     const int wib = threadIdx.x >> 5;
-    double* sgrad = smem;
-    const int ngrad = (DERIV && smem_grad) ? natm * 3 : 0;
     const int per_warp = 32 * ci.item + ci.nr * 3 * ci.gt;
-    double* items = smem + ngrad + wib * per_warp;
+    double* items = smem + wib * per_warp;
     double* gtab = items + 32 * ci.item;
     const long gwarp = (long)blockIdx.x * DFB_WARPS_PER_BLOCK + wib;
     const long nwarps = (long)gridDim.x * DFB_WARPS_PER_BLOCK;
-    double* E = scratch + gwarp * slot;  // U | WA | WB for DERIV, else E
-
-    if (DERIV && smem_grad) {
-        for (int i = threadIdx.x; i < ngrad; i += blockDim.x) sgrad[i] = 0.0;
-        __syncthreads();
-    }
-
-    // Elements (e, f) of the contracted intermediate are split over the lanes,
-    // KB per lane per chunk; large classes loop over several chunks, re-running
-    // the primitive loop for each (their tasks are few).
     const int chunk_elems = 32 * KB;
     const int nchunk = (ci.nef + chunk_elems - 1) / chunk_elems;
     const int M = ci.mmax + 1;
@@ -184,20 +181,21 @@ __global__ void __launch_bounds__(DFB_WARPS_PER_BLOCK * 32)
         }
     };
     if (nchunk == 1) make_offsets(0);
+    const long nunits = nt * nchunk;
 
-    for (long task = gwarp; task < ntask; task += nwarps) {
+    for (long unit = gwarp; unit < nunits; unit += nwarps) {
+        const long tl = unit / nchunk;
+        const int ch = (int)(unit - tl * nchunk);
+        const long task = t0 + tl;
         const long tp = naux_grid > 0 ? task / naux_grid : task;
         const long ta = naux_grid > 0 ? task - tp * naux_grid : task;
         const int pair = task_pair[tp];
         const int C = task_aux[ta];
         const int shA = ps.shA[pair];
-        const int shB = ps.b_dummy ? -1 : ps.shB[pair];
-        double A[3], AB[3], Cc[3];
+        double A[3], Cc[3];
 #pragma unroll
         for (int d = 0; d < 3; ++d) {
             A[d] = ps.cxyz[3 * shA + d];
-            const double Bd = ps.b_dummy ? 0.0 : ps.cxyz[3 * shB + d];
-            AB[d] = A[d] - Bd;
             Cc[d] = ax.cxyz[3 * C + d];
         }
         const int p0 = ps.pstart[pair];
@@ -205,113 +203,154 @@ __global__ void __launch_bounds__(DFB_WARPS_PER_BLOCK * 32)
         const int c0 = ax.pstart[C];
         const int nprimC = ax.nprim[C];
         const long nitems = (long)nprimAB * nprimC;
-
-        if (DERIV) {
-            for (int t = lane; t < 3 * ci.nef; t += 32) E[t] = 0.0;
+        double* E = scratch + tl * slot;
+        const int cbase = ch * chunk_elems;
+        if (nchunk > 1) make_offsets(cbase);
+        double acc[KB];
+#pragma unroll
+        for (int k = 0; k < KB; ++k) {
+            acc[k] = 0.0;
+            if (DERIV && off[k] >= 0) {
+                const int t = cbase + lane + 32 * k;
+                E[t] = 0.0;
+                E[ci.nef + t] = 0.0;
+                E[2 * ci.nef + t] = 0.0;
+            }
         }
 
-        for (int ch = 0; ch < nchunk; ++ch) {
-            const int cbase = ch * chunk_elems;
-            if (nchunk > 1) make_offsets(cbase);
-            double acc[KB];
+        for (long base = 0; base < nitems; base += 32) {
+            const long j = base + lane;
+            if (j < nitems) {
+                const int iab = (int)(j / nprimC);
+                const int ic = (int)(j - (long)iab * nprimC);
+                const double p = ps.eta[p0 + iab];
+                const double Pp[3] = {ps.Px[p0 + iab], ps.Py[p0 + iab], ps.Pz[p0 + iab]};
+                const double q = ax.pexp[c0 + ic];
+                const double inv = 1.0 / (p + q);
+                double PQ2 = 0.0;
+                double* it = items + lane * ci.item;
+                it[0] = p;
+                it[1] = q;
 #pragma unroll
-            for (int k = 0; k < KB; ++k) acc[k] = 0.0;
-
-            for (long base = 0; base < nitems; base += 32) {
-                const long j = base + lane;
-                if (j < nitems) {
-                    const int iab = (int)(j / nprimC);
-                    const int ic = (int)(j - (long)iab * nprimC);
-                    const double p = ps.eta[p0 + iab];
-                    const double Pp[3] = {ps.Px[p0 + iab], ps.Py[p0 + iab], ps.Pz[p0 + iab]};
-                    const double q = ax.pexp[c0 + ic];
+                for (int d = 0; d < 3; ++d) {
+                    const double cp = Cc[d] - Pp[d];
+                    PQ2 += cp * cp;
+                    it[2 + d] = Pp[d] - A[d];
+                    it[5 + d] = cp;
+                }
+                const double T = p * q * inv * PQ2;
+                const double pref = kTwoPi52 / (p * q * sqrt(p + q)) * ps.cK[p0 + iab] * ax.pcoef[c0 + ic];
+                double xr[DFB_NROOTS_MAX], wr[DFB_NROOTS_MAX];
+                rys_eval(tab, ci.nr, T, xr, wr);
+                for (int u = 0; u < ci.nr; ++u) {
+                    it[8 + u] = xr[u];
+                    it[8 + ci.nr + u] = pref * wr[u];
+                }
+            }
+            __syncwarp();
+            const int nb = (int)((nitems - base) < 32 ? (nitems - base) : 32);
+            for (int jj = 0; jj < nb; ++jj) {
+                const double* it = items + jj * ci.item;
+                if (lane < ci.nr * 3) {
+                    const int u = lane / 3, d = lane - 3 * (lane / 3);
+                    const double p = it[0], q = it[1];
                     const double inv = 1.0 / (p + q);
-                    double PQ2 = 0.0;
-                    double* it = items + lane * ci.item;
-                    it[0] = p;
-                    it[1] = q;
+                    const double x = it[8 + u];
+                    const double B0 = x * 0.5 * inv;
+                    const double B1 = (1.0 - x) * 0.5 / p + B0;
+                    const double B1p = (1.0 - x) * 0.5 / q + B0;
+                    const double Cd = it[2 + d] + (q * inv) * x * it[5 + d];
+                    const double Cpd = -(p * inv) * x * it[5 + d];
+                    const double g00 = (d == 0) ? it[8 + ci.nr + u] : 1.0;
+                    build_G(gtab + (u * 3 + d) * ci.gt, ci.nmax, ci.mmax, g00, Cd, Cpd, B0, B1, B1p);
+                }
+                __syncwarp();
 #pragma unroll
-                    for (int d = 0; d < 3; ++d) {
-                        const double cp = Cc[d] - Pp[d];
-                        PQ2 += cp * cp;
-                        it[2 + d] = Pp[d] - A[d];
-                        it[5 + d] = cp;
+                for (int k = 0; k < KB; ++k) {
+                    if (off[k] >= 0) {
+                        const int ox = off[k] & 1023, oy = (off[k] >> 10) & 1023, oz = off[k] >> 20;
+                        double v = 0.0;
+                        for (int u = 0; u < ci.nr; ++u) {
+                            const double* g = gtab + u * 3 * ci.gt;
+                            v = fma(g[ox] * g[ci.gt + oy], g[2 * ci.gt + oz], v);
+                        }
+                        acc[k] += v;
                     }
-                    const double T = p * q * inv * PQ2;
-                    const double pref = kTwoPi52 / (p * q * sqrt(p + q)) * ps.cK[p0 + iab] * ax.pcoef[c0 + ic];
-                    double xr[DFB_NROOTS_MAX], wr[DFB_NROOTS_MAX];
-                    rys_eval(tab, ci.nr, T, xr, wr);
-                    for (int u = 0; u < ci.nr; ++u) {
-                        it[8 + u] = xr[u];
-                        it[8 + ci.nr + u] = pref * wr[u];
+                }
+                if (DERIV) {
+                    const long gidx = base + jj;
+                    if ((gidx + 1) % nprimC == 0) {
+                        const int iab = (int)(gidx / nprimC);
+                        const double a2 = 2.0 * ps.ea[p0 + iab];
+                        const double b2 = 2.0 * ps.eb[p0 + iab];
+#pragma unroll
+                        for (int k = 0; k < KB; ++k) {
+                            const int t = cbase + lane + 32 * k;
+                            if (off[k] >= 0) {
+                                E[t] += acc[k];
+                                E[ci.nef + t] += a2 * acc[k];
+                                E[2 * ci.nef + t] += b2 * acc[k];
+                                acc[k] = 0.0;
+                            }
+                        }
                     }
                 }
                 __syncwarp();
-                const int nb = (int)((nitems - base) < 32 ? (nitems - base) : 32);
-                for (int jj = 0; jj < nb; ++jj) {
-                    const double* it = items + jj * ci.item;
-                    if (lane < ci.nr * 3) {
-                        const int u = lane / 3, d = lane - 3 * (lane / 3);
-                        const double p = it[0], q = it[1];
-                        const double inv = 1.0 / (p + q);
-                        const double x = it[8 + u];
-                        const double B0 = x * 0.5 * inv;
-                        const double B1 = (1.0 - x) * 0.5 / p + B0;
-                        const double B1p = (1.0 - x) * 0.5 / q + B0;
-                        const double Cd = it[2 + d] + (q * inv) * x * it[5 + d];
-                        const double Cpd = -(p * inv) * x * it[5 + d];
-                        const double g00 = (d == 0) ? it[8 + ci.nr + u] : 1.0;
-                        build_G(gtab + (u * 3 + d) * ci.gt, ci.nmax, ci.mmax, g00, Cd, Cpd, B0, B1, B1p);
-                    }
-                    __syncwarp();
-#pragma unroll
-                    for (int k = 0; k < KB; ++k) {
-                        if (off[k] >= 0) {
-                            const int ox = off[k] & 1023, oy = (off[k] >> 10) & 1023, oz = off[k] >> 20;
-                            double v = 0.0;
-                            for (int u = 0; u < ci.nr; ++u) {
-                                const double* g = gtab + u * 3 * ci.gt;
-                                v = fma(g[ox] * g[ci.gt + oy], g[2 * ci.gt + oz], v);
-                            }
-                            acc[k] += v;
-                        }
-                    }
-                    if (DERIV) {
-                        const long gidx = base + jj;
-                        if ((gidx + 1) % nprimC == 0) {
-                            const int iab = (int)(gidx / nprimC);
-                            const double a2 = 2.0 * ps.ea[p0 + iab];
-                            const double b2 = 2.0 * ps.eb[p0 + iab];
-#pragma unroll
-                            for (int k = 0; k < KB; ++k) {
-                                const int t = cbase + lane + 32 * k;
-                                if (off[k] >= 0) {
-                                    E[t] += acc[k];
-                                    E[ci.nef + t] += a2 * acc[k];
-                                    E[2 * ci.nef + t] += b2 * acc[k];
-                                    acc[k] = 0.0;
-                                }
-                            }
-                        }
-                    }
-                    __syncwarp();
-                }
             }
-            if (!DERIV) {
+        }
+        if (!DERIV) {
 #pragma unroll
-                for (int k = 0; k < KB; ++k) {
-                    if (off[k] >= 0) E[cbase + lane + 32 * k] = acc[k];
-                }
+            for (int k = 0; k < KB; ++k) {
+                if (off[k] >= 0) E[cbase + lane + 32 * k] = acc[k];
             }
         }
         __syncwarp();
+    }
+}
 
+#define DFB_EPI_CHUNK 128  // tile elements per epilogue work unit
+
+// Phase 2: one warp per (task, tile chunk) -- horizontal recurrence from the task's scratch
+// slot, then the tile goes to its final place (integrals) or is contracted with
+// the adjoint (derivative; per-block partial gradients in shared memory).
+template <bool DERIV>
+__global__ void __launch_bounds__(DFB_WARPS_PER_BLOCK * 32)
+    k_rys_epi(ClassInfo ci, dfb_pair_side_t ps, dfb_aux_side_t ax, const int* __restrict__ task_pair,
+              const int* __restrict__ task_aux, long t0, long nt, long naux_grid, int mode, double* __restrict__ out,
+              long sP, long sM, long sN, const double* __restrict__ bar, long sbP, long sbM, long sbN,
+              double* __restrict__ grad, int natm, int smem_grad, const double* __restrict__ scratch, long slot) {
+    extern __shared__ double sgrad[];
+    const int lane = threadIdx.x & 31;
+    const int wib = threadIdx.x >> 5;
+    const int ngrad = (DERIV && smem_grad) ? natm * 3 : 0;
+    const long gwarp = (long)blockIdx.x * DFB_WARPS_PER_BLOCK + wib;
+    const long nwarps = (long)gridDim.x * DFB_WARPS_PER_BLOCK;
+    if (DERIV && smem_grad) {
+        for (int i = threadIdx.x; i < ngrad; i += blockDim.x) sgrad[i] = 0.0;
+        __syncthreads();
+    }
+    const int ntile = ci.na * ci.nb * ci.nc;
+    const int nec = (ntile + DFB_EPI_CHUNK - 1) / DFB_EPI_CHUNK;
+    for (long unit = gwarp; unit < nt * nec; unit += nwarps) {
+        const long tl = unit / nec;
+        const int i0 = (int)(unit - tl * nec) * DFB_EPI_CHUNK;
+        const int i1 = (i0 + DFB_EPI_CHUNK < ntile) ? i0 + DFB_EPI_CHUNK : ntile;
+        const long task = t0 + tl;
+        const long tp = naux_grid > 0 ? task / naux_grid : task;
+        const long ta = naux_grid > 0 ? task - tp * naux_grid : task;
+        const int pair = task_pair[tp];
+        const int C = task_aux[ta];
+        const int shA = ps.shA[pair];
+        const int shB = ps.b_dummy ? -1 : ps.shB[pair];
+        double AB[3];
+#pragma unroll
+        for (int d = 0; d < 3; ++d) AB[d] = ps.cxyz[3 * shA + d] - (ps.b_dummy ? 0.0 : ps.cxyz[3 * shB + d]);
+        const double* E = scratch + tl * slot;
         const int aoA = ps.aostart[shA];
         const int aoB = ps.b_dummy ? 0 : ps.aostart[shB];
         const int aoC = ax.aostart[C];
-        const int ntile = ci.na * ci.nb * ci.nc;
         double gA[3] = {0.0, 0.0, 0.0}, gB[3] = {0.0, 0.0, 0.0};
-        for (int idx = lane; idx < ntile; idx += 32) {
+        for (int idx = i0 + lane; idx < i1; idx += 32) {
             const int ic = idx % ci.nc;
             const int iab = idx / ci.nc;
             const int ib = iab % ci.nb;
@@ -391,7 +430,6 @@ __global__ void __launch_bounds__(DFB_WARPS_PER_BLOCK * 32)
         }
         __syncwarp();
     }
-
     if (DERIV && smem_grad) {
         __syncthreads();
         for (int i = threadIdx.x; i < ngrad; i += blockDim.x)
@@ -461,6 +499,11 @@ static int current_device() {
     return dev;
 }
 
+// Scratch policy of the generic path: one slot (nef or 3 nef doubles) per task
+// of a batch; batches of up to DFB_SCRATCH_TASKS tasks, or fewer when the
+// caller's scratch is smaller (the fixed scratch of dfb_rys_int_noalloc).
+#define DFB_SCRATCH_TASKS 16384L
+
 template <int KB, bool DERIV>
 static int launch_rys(const ClassInfo& ci, const dfb_pair_side_t* ps, const dfb_aux_side_t* ax,
                       const int* task_pair, const int* task_aux, long ntask, long naux_grid, int mode, double* out,
@@ -468,56 +511,52 @@ static int launch_rys(const ClassInfo& ci, const dfb_pair_side_t* ps, const dfb_
                       double* scratch, long scratch_doubles, cudaStream_t st, int query_only, long* need,
                       int fit_grid_to_scratch = 0) {
     const int dev = current_device();
-    const int smem_grad = (DERIV && natm * 3 <= 4096) ? 1 : 0;
-    const size_t smem =
-        sizeof(double) * ((DERIV && smem_grad ? natm * 3 : 0) +
-                          (size_t)DFB_WARPS_PER_BLOCK * (32 * ci.item + ci.nr * 3 * ci.gt));
-    auto kern = k_rys<KB, DERIV>;
-    if (smem > 48 * 1024) {
-        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        if (e != cudaSuccess) return set_cuda_error("cudaFuncSetAttribute", e);
-    }
-    // The persistent grid (and so the scratch size) is sized from the occupancy
-    // without the optional per-block gradient buffer, so that the scratch
-    // requirement does not depend on the atom count.
-    const size_t smem_base = sizeof(double) * ((size_t)DFB_WARPS_PER_BLOCK * (32 * ci.item + ci.nr * 3 * ci.gt));
-    if (smem_base > 48 * 1024 && smem <= 48 * 1024) {
-        cudaError_t e0 = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_base);
-        if (e0 != cudaSuccess) return set_cuda_error("cudaFuncSetAttribute", e0);
-    }
-    int occ = 0;
-    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, DFB_WARPS_PER_BLOCK * 32, smem_base);
-    if (e != cudaSuccess) return set_cuda_error("occupancy", e);
-    if (occ < 1) return set_error(DFB_ERR_UNSUPPORTED, "class (%d,%d,%d) does not fit on an SM", ci.la, ci.lb, ci.lc);
-    int nsm = 0;
-    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    long blocks_needed = (ntask + DFB_WARPS_PER_BLOCK - 1) / DFB_WARPS_PER_BLOCK;
-    long blocks = (long)occ * nsm;
-    if (blocks > blocks_needed) blocks = blocks_needed;
-    if (blocks < 1) blocks = 1;
     const long slot = (DERIV ? 3L : 1L) * ci.nef;
-    if (fit_grid_to_scratch) {
-        // fixed scratch: shrink the persistent grid until its warp slots fit
-        const long fit = scratch_doubles / (DFB_WARPS_PER_BLOCK * slot);
-        if (fit < 1)
-            return set_error(DFB_ERR_UNSUPPORTED,
-                             "class (%d,%d,%d) needs %ld scratch doubles per block, the fixed scratch holds %ld",
-                             ci.la, ci.lb, ci.lc, (long)DFB_WARPS_PER_BLOCK * slot, scratch_doubles);
-        if (blocks > fit) blocks = fit;
-    }
-    const long required = blocks * DFB_WARPS_PER_BLOCK * slot;
     if (query_only) {
-        *need = required;
+        *need = (ntask < DFB_SCRATCH_TASKS ? (ntask > 0 ? ntask : 1) : DFB_SCRATCH_TASKS) * slot;
         return DFB_OK;
     }
     if (ntask == 0) return DFB_OK;
-    if (scratch == nullptr || scratch_doubles < required)
-        return set_error(DFB_ERR_INVALID, "scratch too small: need %ld doubles, got %ld", required, scratch_doubles);
-    kern<<<(unsigned)blocks, DFB_WARPS_PER_BLOCK * 32, smem, st>>>(
-        ci, *ps, *ax, task_pair, task_aux, ntask, naux_grid, mode, out, sP, sM, sN, bar, sbP, sbM, sbN, grad, natm, smem_grad,
-        scratch, slot, g_tables[dev].tab);
-    e = cudaGetLastError();
-    if (e != cudaSuccess) return set_cuda_error("k_rys launch", e);
+    if (scratch == nullptr || scratch_doubles < slot)
+        return set_error(fit_grid_to_scratch ? DFB_ERR_UNSUPPORTED : DFB_ERR_INVALID,
+                         "class (%d,%d,%d) needs %ld scratch doubles per task, the scratch holds %ld", ci.la, ci.lb,
+                         ci.lc, slot, scratch_doubles);
+    const int smem_grad = (DERIV && natm * 3 <= 4096) ? 1 : 0;
+    const size_t smem_acc = sizeof(double) * ((size_t)DFB_WARPS_PER_BLOCK * (32 * ci.item + ci.nr * 3 * ci.gt));
+    const size_t smem_epi = smem_grad ? sizeof(double) * natm * 3 : 0;
+    auto kacc = k_rys_acc<KB, DERIV>;
+    auto kepi = k_rys_epi<DERIV>;
+    if (smem_acc > 48 * 1024) {
+        cudaError_t e = cudaFuncSetAttribute(kacc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_acc);
+        if (e != cudaSuccess) return set_cuda_error("cudaFuncSetAttribute", e);
+    }
+    int occ_acc = 0, occ_epi = 0, nsm = 0;
+    cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_acc, kacc, DFB_WARPS_PER_BLOCK * 32, smem_acc);
+    if (e == cudaSuccess)
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_epi, kepi, DFB_WARPS_PER_BLOCK * 32, smem_epi);
+    if (e != cudaSuccess) return set_cuda_error("occupancy", e);
+    if (occ_acc < 1 || occ_epi < 1)
+        return set_error(DFB_ERR_UNSUPPORTED, "class (%d,%d,%d) does not fit on an SM", ci.la, ci.lb, ci.lc);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    const int nchunk = (ci.nef + 32 * KB - 1) / (32 * KB);
+    const long batch = scratch_doubles / slot;
+    for (long t0 = 0; t0 < ntask; t0 += batch) {
+        const long nt = (ntask - t0) < batch ? (ntask - t0) : batch;
+        long b1 = (nt * nchunk + DFB_WARPS_PER_BLOCK - 1) / DFB_WARPS_PER_BLOCK;
+        if (b1 > (long)occ_acc * nsm) b1 = (long)occ_acc * nsm;
+        kacc<<<(unsigned)b1, DFB_WARPS_PER_BLOCK * 32, smem_acc, st>>>(ci, *ps, *ax, task_pair, task_aux, t0, nt,
+                                                                          naux_grid, scratch, slot,
+                                                                          g_tables[dev].tab);
+        const long nec = (ci.na * ci.nb * ci.nc + DFB_EPI_CHUNK - 1) / DFB_EPI_CHUNK;
+        long b2 = (nt * nec + DFB_WARPS_PER_BLOCK - 1) / DFB_WARPS_PER_BLOCK;
+        if (b2 > (long)occ_epi * nsm) b2 = (long)occ_epi * nsm;
+        kepi<<<(unsigned)b2, DFB_WARPS_PER_BLOCK * 32, smem_epi, st>>>(ci, *ps, *ax, task_pair, task_aux, t0, nt,
+                                                                          naux_grid, mode, out, sP, sM, sN, bar, sbP,
+                                                                          sbM, sbN, grad, natm, smem_grad, scratch,
+                                                                          slot);
+        e = cudaGetLastError();
+        if (e != cudaSuccess) return set_cuda_error("k_rys launch", e);
+    }
     return DFB_OK;
 }
 
@@ -549,6 +588,10 @@ static int dispatch_rys(int la, int lb, int lc, const dfb_pair_side_t* ps, const
             }
         cudaError_t e = cudaMemcpyToSymbol(c_binomtab, h, sizeof(h));
         if (e != cudaSuccess) return set_cuda_error("binomial table upload", e);
+        int nb[2 * DFB_LMAX + 4];
+        for (int L = 0; L < 2 * DFB_LMAX + 4; ++L) nb[L] = ncart_below(L);
+        e = cudaMemcpyToSymbol(c_ncbtab, nb, sizeof(nb));
+        if (e != cudaSuccess) return set_cuda_error("index table upload", e);
         g_binom_ready[dev] = true;
     }
     if (!query_only && ntask > 0 && getenv("DFB_DISABLE_TMPL") == nullptr) {
@@ -572,7 +615,7 @@ static int dispatch_rys(int la, int lb, int lc, const dfb_pair_side_t* ps, const
         g.natm = natm;
         g.smem_grad = (DERIV && natm * 3 <= 4096) ? 1 : 0;
         g.tab = g_tables[dev].tab;
-        const size_t smem = g.smem_grad ? sizeof(double) * natm * 3 : 0;
+        const size_t smem = (g.smem_grad ? sizeof(double) * natm * 3 : 0) + sizeof(double) * 128 * 2 * ci.nr;
         const long nblk = (ntask + 127) / 128;
         if (nblk > 2147483647L) return set_error(DFB_ERR_INVALID, "too many tasks in one class launch");
         if (tmpl_launch(la, lb, lc, DERIV, g, nblk, smem, st)) {
@@ -580,6 +623,10 @@ static int dispatch_rys(int la, int lb, int lc, const dfb_pair_side_t* ps, const
             if (e != cudaSuccess) return set_cuda_error("k_rys_thread launch", e);
             return DFB_OK;
         }
+    }
+    if (query_only && getenv("DFB_DISABLE_TMPL") == nullptr && tmpl_has(la, lb, lc, DERIV)) {
+        *need = 0;
+        return DFB_OK;
     }
     const int kb = (ci.nef + 31) / 32;
 #define DFB_CASE(K)                                                                                              \

@@ -113,6 +113,50 @@ __device__ __forceinline__ void rys_eval_t(const RysTable& tab, double T, double
     }
 }
 
+// Same evaluation, two table functions at a time, results to a per-thread
+// shared-memory slot r[0..NR) = nodes, r[NR..2NR) = weights (bounds the
+// coefficient registers in flight).
+template <int NR>
+__device__ __forceinline__ void rys_eval_smem(const RysTable& tab, double T, double* __restrict__ r) {
+    if (T >= tab.tmax) {
+        const double* h = tab.herm + tab.hoff[NR];
+        const double inv = 1.0 / T;
+        const double rs = rsqrt(T);
+#pragma unroll
+        for (int i = 0; i < NR; ++i) {
+            r[i] = __ldg(h + i) * inv;
+            r[NR + i] = __ldg(h + NR + i) * rs;
+        }
+        return;
+    }
+    int k = (int)T;
+    if (k > tab.nint - 1) k = tab.nint - 1;
+    const double u = 2.0 * (T - (double)k) - 1.0;
+    constexpr int S = DFB_RYS_DEG + 1;
+    const double2* c = reinterpret_cast<const double2*>(tab.coef + tab.offs[NR] + (size_t)k * (2 * NR) * S);
+#pragma unroll 1
+    for (int f = 0; f < 2 * NR; f += 2) {
+        double cf0[S], cf1[S];
+#pragma unroll
+        for (int d = 0; d < S / 2; ++d) {
+            const double2 v0 = __ldg(c + f * (S / 2) + d);
+            const double2 v1 = __ldg(c + (f + 1) * (S / 2) + d);
+            cf0[2 * d] = v0.x;
+            cf0[2 * d + 1] = v0.y;
+            cf1[2 * d] = v1.x;
+            cf1[2 * d + 1] = v1.y;
+        }
+        double a0 = cf0[S - 1], a1 = cf1[S - 1];
+#pragma unroll
+        for (int d = S - 2; d >= 0; --d) {
+            a0 = fma(a0, u, cf0[d]);
+            a1 = fma(a1, u, cf1[d]);
+        }
+        r[f] = a0;
+        r[f + 1] = a1;
+    }
+}
+
 template <int NM, int MM>
 __device__ __forceinline__ void build_G_t(double (&G)[NM + 1][MM + 1], double g00, double C, double Cp, double B0,
                                           double B1, double B1p) {
@@ -370,6 +414,9 @@ struct Cls {
 template <class CL>
 __device__ __forceinline__ void rys_thread_body(const TmplArgs& g, long task, double* sgrad) {
     constexpr int NR = CL::NR, NM = CL::NM, LB = CL::LB;
+    // per-thread root slot after the optional gradient buffer
+    extern __shared__ double smem_all[];
+    double* sroot = smem_all + ((CL::DERIV && g.smem_grad) ? g.natm * 3 : 0) + threadIdx.x * (2 * NR);
     const long tp = g.naux_grid > 0 ? task / g.naux_grid : task;
     const long ta = g.naux_grid > 0 ? task - tp * g.naux_grid : task;
     const int pair = g.task_pair[tp];
@@ -412,20 +459,32 @@ __device__ __forceinline__ void rys_thread_body(const TmplArgs& g, long task, do
             const double inv = 1.0 / (p + q);
             const double T = p * q * inv * PQ2;
             const double pref = kTwoPi52_t / (p * q * sqrt(p + q)) * cK * cc;
-            double xr[NR], wr[NR];
-            rys_eval_t<NR>(g.tab, T, xr, wr);
+            // few roots: registers; more roots: shared-memory slot (bounds registers)
+            constexpr int NRR = NR <= 2 ? NR : 1;
+            double xr[NRR], wr[NRR];
+            if constexpr (NR <= 2)
+                rys_eval_t<NR>(g.tab, T, xr, wr);
+            else
+                rys_eval_smem<NR>(g.tab, T, sroot);
             const double qi = q * inv, pi = p * inv;
             const double h_p = 0.5 / p, h_q = 0.5 / q;
 #pragma unroll
             for (int u = 0; u < NR; ++u) {
-                const double x = xr[u];
+                double x, wu;
+                if constexpr (NR <= 2) {
+                    x = xr[u < NRR ? u : 0];
+                    wu = wr[u < NRR ? u : 0];
+                } else {
+                    x = sroot[u];
+                    wu = sroot[NR + u];
+                }
                 const double B0 = x * 0.5 * inv;
                 const double B1 = (1.0 - x) * h_p + B0;
                 const double B1p = (1.0 - x) * h_q + B0;
                 typename CL::GtX Gx;
                 typename CL::GtY Gy;
                 typename CL::GtZ Gz;
-                build_G_t<NM, CL::MDX>(Gx, pref * wr[u], PA[0] + qi * x * CP[0], -pi * x * CP[0], B0, B1, B1p);
+                build_G_t<NM, CL::MDX>(Gx, pref * wu, PA[0] + qi * x * CP[0], -pi * x * CP[0], B0, B1, B1p);
                 build_G_t<NM, CL::MDY>(Gy, 1.0, PA[1] + qi * x * CP[1], -pi * x * CP[1], B0, B1, B1p);
                 build_G_t<NM, CL::MDZ>(Gz, 1.0, PA[2] + qi * x * CP[2], -pi * x * CP[2], B0, B1, B1p);
                 CL::acc_all(acc, Gx, Gy, Gz, a2, b2);

@@ -120,7 +120,18 @@ def main() -> None:
         d = name[8] == "d"
         la = int(name[9:])
         hdr.append(f"    if ({'deriv' if d else '!deriv'} && la == {la}) return {name}_launch(la, lb, lc, g, nblk, smem, st);")
-    hdr += ["    return 0;", "}", "}  // namespace dfb", ""]
+    hdr += ["    return 0;", "}", ""]
+    # host-side query: is a class served by a specialised kernel?
+    hdr.append("inline bool tmpl_has(int la, int lb, int lc, bool deriv) {")
+    for deriv in (False, True):
+        keys = [f"({la}, {lb}, {lc})" for la in range(LA_MAX + 1) for lb in range(la + 1) for lc in range(LC_MAX + 1)
+                if plan(la, lb, lc, deriv) is not None]
+        hdr.append(f"    static const int k{'d' if deriv else 'i'}[][3] = {{{', '.join('{' + k[1:-1] + '}' for k in keys)}}};")
+    hdr += ["    const int (*k)[3] = deriv ? kd : ki;",
+            "    const int n = deriv ? (int)(sizeof(kd) / sizeof(kd[0])) : (int)(sizeof(ki) / sizeof(ki[0]));",
+            "    for (int i = 0; i < n; ++i)",
+            "        if (k[i][0] == la && k[i][1] == lb && k[i][2] == lc) return true;",
+            "    return false;", "}", "}  // namespace dfb", ""]
     with open(os.path.join(HERE, "dfb_cls_dispatch.h"), "w") as f:
         f.write("\n".join(hdr))
     print("generated", len(groups), "groups")
