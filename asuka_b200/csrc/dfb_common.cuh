@@ -19,8 +19,9 @@ __host__ __device__ __forceinline__ int cart_index(int ex, int ey, int l) {
     return ((l - ex) * (l - ex + 1)) / 2 + (l - ex - ey);
 }
 
-// Rys root/weight table: per root count n, NINT unit intervals in T, 2n rows
-// (n nodes then n weights), DEG+1 power-basis coefficients in u = 2(T-k)-1.
+// Rys root/weight table: per root count n, NINT equal intervals of T in
+// [0, tmax), 2n rows (n nodes then n weights), DEG+1 power-basis coefficients
+// in u = 2(T/h - k) - 1, h = tmax/NINT.
 struct RysTable {
     const double* coef;   // concatenated over n = 1..nmax
     const double* herm;   // per n: s_i^2 (n) then W_i (n), concatenated
@@ -28,6 +29,7 @@ struct RysTable {
     int hoff[DFB_NROOTS_MAX + 1];   // hermite offset of root count n
     int nmax, nint, deg;
     double tmax;
+    double inv_h;  // intervals per unit T (nint / tmax)
 };
 
 // Nodes x_i (in t^2) and weights w_i (sum w_i = F_0(T)) of the n-point Rys rule.
@@ -42,9 +44,10 @@ __device__ __forceinline__ void rys_eval(const RysTable& tab, int n, double T, d
         }
         return;
     }
-    int k = (int)T;
+    const double Th = T * tab.inv_h;
+    int k = (int)Th;
     if (k > tab.nint - 1) k = tab.nint - 1;
-    const double u = 2.0 * (T - (double)k) - 1.0;
+    const double u = 2.0 * (Th - (double)k) - 1.0;
     const int stride = tab.deg + 1;
     const double* c = tab.coef + tab.offs[n] + (size_t)k * (2 * n) * stride;
     for (int r = 0; r < 2 * n; ++r) {

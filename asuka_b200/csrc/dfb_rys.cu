@@ -675,6 +675,7 @@ extern "C" int dfb_rys_table_init(const double* coef, const int* offs, long ncoe
     t.tab.nint = nint;
     t.tab.deg = deg;
     t.tab.tmax = tmax;
+    t.tab.inv_h = (double)nint / tmax;
     t.ready = true;
     return DFB_OK;
 }

@@ -26,7 +26,7 @@
 #include "../../include/dfb.h"
 #include "dfb_common.cuh"
 
-#define DFB_RYS_DEG 15  // Horner degree of the Rys table (checked at upload)
+#define DFB_RYS_DEG 9  // Horner degree of the Rys table (checked at upload)
 
 namespace dfb {
 
@@ -89,9 +89,10 @@ __device__ __forceinline__ void rys_eval_t(const RysTable& tab, double T, double
         }
         return;
     }
-    int k = (int)T;
+    const double Th = T * tab.inv_h;
+    int k = (int)Th;
     if (k > tab.nint - 1) k = tab.nint - 1;
-    const double u = 2.0 * (T - (double)k) - 1.0;
+    const double u = 2.0 * (Th - (double)k) - 1.0;
     constexpr int S = DFB_RYS_DEG + 1;
     const double2* c = reinterpret_cast<const double2*>(tab.coef + tab.offs[NR] + (size_t)k * (2 * NR) * S);
 #pragma unroll
@@ -129,9 +130,10 @@ __device__ __forceinline__ void rys_eval_smem(const RysTable& tab, double T, dou
         }
         return;
     }
-    int k = (int)T;
+    const double Th = T * tab.inv_h;
+    int k = (int)Th;
     if (k > tab.nint - 1) k = tab.nint - 1;
-    const double u = 2.0 * (T - (double)k) - 1.0;
+    const double u = 2.0 * (Th - (double)k) - 1.0;
     constexpr int S = DFB_RYS_DEG + 1;
     const double2* c = reinterpret_cast<const double2*>(tab.coef + tab.offs[NR] + (size_t)k * (2 * NR) * S);
 #pragma unroll 1

@@ -13,8 +13,8 @@ monomial Stieltjes procedure and a QL eigensolve
 in 100-digit arithmetic (mpmath): moments F_m(T) = 1F1(m+1/2; m+3/2; -T)/(2m+1),
 Jacobi matrix by the Chebyshev algorithm on the moments, eigen-decomposition
 (Golub-Welsch).  Each node/weight is then fitted on T in [0, T_MAX) by a
-degree-``DEG`` Chebyshev interpolant per unit interval, stored in the power
-basis of the local variable u = 2(T - T0) - 1 for Horner evaluation.
+degree-``DEG`` Chebyshev interpolant per interval of width T_MAX/NINT, stored in the power
+basis of the local variable u = 2(T - T0)/h - 1 for Horner evaluation.
 
 For T >= T_MAX the Gauss-Hermite limit is exact to the working precision:
 x_i = s_i^2 / T, w_i = W_i / sqrt(T), with s_i > 0 the positive roots of
@@ -37,8 +37,8 @@ import numpy as np
 
 NMAX = 10
 T_MAX = 96.0
-NINT = 96          # unit intervals on [0, T_MAX)
-DEG = 15
+NINT = 192         # intervals of width 0.5 on [0, T_MAX)
+DEG = 9
 DPS = 110
 
 
@@ -107,9 +107,10 @@ def _fit_interval(args):
     us_f = np.array([float(u) for u in us])
     V = np.polynomial.chebyshev.chebvander(us_f, DEG)  # (npts, DEG+1)
     cheb = np.linalg.solve(V, vals)  # (DEG+1, 2n)
-    power = np.stack([np.polynomial.chebyshev.cheb2poly(cheb[:, i]) for i in range(2 * n)])
     out = np.zeros((2 * n, DEG + 1))
-    out[:, : power.shape[1]] = power
+    for i in range(2 * n):
+        pw = np.polynomial.chebyshev.cheb2poly(cheb[:, i])
+        out[i, : pw.size] = pw
     return n, k, out
 
 

@@ -36,6 +36,7 @@ from .basis import BasisCartSoA, build_shell_pairs_l_order, from_reference_like,
 _DATA = os.path.join(os.path.dirname(os.path.abspath(__file__)), "data")
 _TABLE_READY: set[int] = set()
 PRIM_SCREEN = 1e-20  # primitive-pair magnitude bound below which a pair is skipped (0 = evaluate all)
+NSTREAMS = int(os.environ.get("DFB_STREAMS", "4"))  # side streams for per-class launches
 NROOTS_SLOTS = 11  # DFB_NROOTS_MAX + 1
 
 
@@ -162,6 +163,32 @@ class DFEngine:
         self._build_ao_pairs(ao.shell_cxyz)
         self._build_pair_tables()
 
+    # ------------------------------------------------------------ class launches over streams
+    def _streams(self):
+        """Side streams for class launches: classes write disjoint outputs (or add to the
+        gradient atomically), so their kernels may overlap and fill each other's tails."""
+        if getattr(self, "_side", None) is None:
+            self._side = [torch.cuda.Stream(device=self.device) for _ in range(NSTREAMS)]
+        return self._side
+
+    def _fanout(self, launches):
+        """Run launch(stream_ptr) callables round-robin over side streams, ordered after and
+        before the current stream."""
+        main = torch.cuda.current_stream(self.device)
+        side = self._streams() if NSTREAMS > 1 else [main]
+        if NSTREAMS > 1:
+            start = torch.cuda.Event()
+            start.record(main)
+            for st in side:
+                st.wait_event(start)
+        for i, fn in enumerate(launches):
+            fn(int(side[i % len(side)].cuda_stream))
+        if NSTREAMS > 1:
+            for st in side:
+                ev = torch.cuda.Event()
+                ev.record(st)
+                main.wait_event(ev)
+
     @property
     def _i32(self):
         return lambda a: torch.as_tensor(np.ascontiguousarray(a, dtype=np.int32), device=self.device)
@@ -260,7 +287,14 @@ class DFEngine:
         self.ax_cxyz.copy_(coords.index_select(0, self.ax_atom.long()))
         self._build_pair_tables()
 
-    def _scratch_for(self, deriv: bool) -> torch.Tensor:
+    def _scratch_for(self, deriv: bool, copies: int = 1) -> torch.Tensor:
+        key = (deriv, os.environ.get("DFB_DISABLE_TMPL"), id(self.classes3c))
+        cache = self.__dict__.setdefault("_need_cache", {})
+        if key in cache:
+            need = cache[key] * copies
+            if self._scratch is None or self._scratch.numel() < need:
+                self._scratch = torch.empty(need, dtype=torch.float64, device=self.device)
+            return self._scratch[:need]
         L = _lib.lib()
         need = 1
         for la, lb, lc, pairs, auxs in self.classes3c:
@@ -271,9 +305,11 @@ class DFEngine:
             n = L.dfb_rys_scratch_doubles(lp, 0, lq, P.numel(), int(deriv))
             _lib.check(0 if n >= 0 else int(n), "dfb_rys_scratch_doubles")
             need = max(need, n)
+        cache[key] = need
+        need *= copies
         if self._scratch is None or self._scratch.numel() < need:
             self._scratch = torch.empty(need, dtype=torch.float64, device=self.device)
-        return self._scratch
+        return self._scratch[:need]
 
     def aux_blocks(self, max_naux: int = 256):
         """Contiguous aux-shell blocks of at most ``max_naux`` functions, aligned to shells
@@ -325,17 +361,54 @@ class DFEngine:
             _lib.check(rc, f"dfb_rys_int 3c block ({la},{lb},{lc})")
         return X
 
+    def _scratch_slices(self, deriv: bool):
+        """Scratch for the generic kernels: one slice per side stream (launches overlap)."""
+        n = max(NSTREAMS, 1)
+        buf = self._scratch_for(deriv, copies=n)
+        per = buf.numel() // n
+        return [buf[i * per:(i + 1) * per] for i in range(n)]
+
+    def _launch_int(self, la, lb, lc, ps, axs, pairs, auxs, ntask, ngrid, mode, out, strides):
+        L = _lib.lib()
+        key = (la, lb, lc, mode)
+
+        def fn(stream, _k=key):
+            i = self._slot_of(stream)
+            scr = self._slices_int[i]
+            rc = L.dfb_rys_int(la, lb, lc, ctypes.byref(ps), ctypes.byref(axs), _lib.ptr(pairs), _lib.ptr(auxs),
+                               ntask, ngrid, mode, _lib.ptr(out), *strides, _lib.ptr(scr), scr.numel(), stream)
+            _lib.check(rc, f"dfb_rys_int {_k}")
+        return fn
+
+    def _launch_deriv(self, la, lb, lc, ps, axs, pairs, auxs, ntask, ngrid, mode, bar, strides, grad):
+        L = _lib.lib()
+        key = (la, lb, lc, mode)
+
+        def fn(stream, _k=key):
+            i = self._slot_of(stream)
+            scr = self._slices_der[i]
+            rc = L.dfb_rys_deriv(la, lb, lc, ctypes.byref(ps), ctypes.byref(axs), _lib.ptr(pairs), _lib.ptr(auxs),
+                                 ntask, ngrid, mode, _lib.ptr(bar), *strides, _lib.ptr(grad), self.natm,
+                                 _lib.ptr(scr), scr.numel(), stream)
+            _lib.check(rc, f"dfb_rys_deriv {_k}")
+        return fn
+
+    def _slot_of(self, stream_ptr: int) -> int:
+        if NSTREAMS <= 1:
+            return 0
+        for i, st in enumerate(self._streams()):
+            if int(st.cuda_stream) == stream_ptr:
+                return i
+        return 0
+
     # ------------------------------------------------------------ integrals
     def metric(self, out: torch.Tensor | None = None) -> torch.Tensor:
         """V[P, Q] = (P|Q), full symmetric (naux, naux)."""
         naux = self.naux
         V = out if out is not None else torch.empty((naux, naux), dtype=torch.float64, device=self.device)
-        scr = self._scratch_for(False)
-        L = _lib.lib()
-        for lp, lq, P, Q in self.classes2c:
-            rc = L.dfb_rys_int(lp, 0, lq, ctypes.byref(self.ps_aux), ctypes.byref(self.axs), _lib.ptr(P), _lib.ptr(Q),
-                               P.numel(), 0, 1, _lib.ptr(V), naux, 1, 0, _lib.ptr(scr), scr.numel(), _stream())
-            _lib.check(rc, f"dfb_rys_int metric ({lp},{lq})")
+        self._slices_int = self._scratch_slices(False)
+        self._fanout([self._launch_int(lp, 0, lq, self.ps_aux, self.axs, P, Q, P.numel(), 0, 1, V, (naux, 1, 0))
+                      for lp, lq, P, Q in self.classes2c])
         # diagonal shell blocks are written from one tile in both orders; make V
         # exactly symmetric as the reference does (cueri_df_cpu.py: V = (V+V^T)/2)
         V.copy_(0.5 * (V + V.T))
@@ -353,13 +426,9 @@ class DFEngine:
         X = out if out is not None else torch.empty(shape, dtype=torch.float64, device=self.device)
         if self.n_dropped_pairs:
             X.zero_()
-        scr = self._scratch_for(False)
-        L = _lib.lib()
-        for la, lb, lc, pairs, auxs in self.classes3c:
-            rc = L.dfb_rys_int(la, lb, lc, ctypes.byref(self.ps_ao), ctypes.byref(self.axs), _lib.ptr(pairs),
-                               _lib.ptr(auxs), pairs.numel() * auxs.numel(), auxs.numel(), 0, _lib.ptr(X), *s,
-                               _lib.ptr(scr), scr.numel(), _stream())
-            _lib.check(rc, f"dfb_rys_int 3c ({la},{lb},{lc})")
+        self._slices_int = self._scratch_slices(False)
+        self._fanout([self._launch_int(la, lb, lc, self.ps_ao, self.axs, pairs, auxs, pairs.numel() * auxs.numel(),
+                                       auxs.numel(), 0, X, s) for la, lb, lc, pairs, auxs in self.classes3c])
         return X
 
     def deriv3c(self, bar: torch.Tensor, grad: torch.Tensor, layout: str = "Qmn") -> torch.Tensor:
@@ -372,26 +441,18 @@ class DFEngine:
         else:
             raise ValueError("layout must be 'Qmn' or 'mnQ'")
         bar = bar.contiguous()
-        scr = self._scratch_for(True)
-        L = _lib.lib()
-        for la, lb, lc, pairs, auxs in self.classes3c:
-            rc = L.dfb_rys_deriv(la, lb, lc, ctypes.byref(self.ps_ao), ctypes.byref(self.axs), _lib.ptr(pairs),
-                                 _lib.ptr(auxs), pairs.numel() * auxs.numel(), auxs.numel(), 0, _lib.ptr(bar), *s,
-                                 _lib.ptr(grad), self.natm, _lib.ptr(scr), scr.numel(), _stream())
-            _lib.check(rc, f"dfb_rys_deriv 3c ({la},{lb},{lc})")
+        self._slices_der = self._scratch_slices(True)
+        self._fanout([self._launch_deriv(la, lb, lc, self.ps_ao, self.axs, pairs, auxs, pairs.numel() * auxs.numel(),
+                                         auxs.numel(), 0, bar, s, grad) for la, lb, lc, pairs, auxs in self.classes3c])
         return grad
 
     def deriv2c(self, bar: torch.Tensor, grad: torch.Tensor) -> torch.Tensor:
         """grad += sum_{P,Q} bar[P,Q] d(P|Q)/dR; bar symmetric."""
         naux = self.naux
         bar = bar.contiguous()
-        scr = self._scratch_for(True)
-        L = _lib.lib()
-        for lp, lq, P, Q in self.classes2c:
-            rc = L.dfb_rys_deriv(lp, 0, lq, ctypes.byref(self.ps_aux), ctypes.byref(self.axs), _lib.ptr(P),
-                                 _lib.ptr(Q), P.numel(), 0, 1, _lib.ptr(bar), naux, 1, 0, _lib.ptr(grad), self.natm,
-                                 _lib.ptr(scr), scr.numel(), _stream())
-            _lib.check(rc, f"dfb_rys_deriv metric ({lp},{lq})")
+        self._slices_der = self._scratch_slices(True)
+        self._fanout([self._launch_deriv(lp, 0, lq, self.ps_aux, self.axs, P, Q, P.numel(), 0, 1, bar, (naux, 1, 0),
+                                         grad) for lp, lq, P, Q in self.classes2c])
         return grad
 
 
