@@ -32,6 +32,23 @@ struct RysTable {
     double inv_h;  // intervals per unit T (nint / tmax)
 };
 
+// Task t -> (pair list index, aux list index).  grid > 0: pair-major grid with
+// `grid` aux shells per pair; grid < 0: aux-major grid with -grid pairs per aux
+// shell (a warp then shares one aux shell and walks consecutive pairs, which the
+// caller sorts by primitive-pair count); grid == 0: explicit lists.
+__device__ __forceinline__ void task_indices(long t, long grid, long& tp, long& ta) {
+    if (grid > 0) {
+        tp = t / grid;
+        ta = t - tp * grid;
+    } else if (grid < 0) {
+        ta = t / (-grid);
+        tp = t - ta * (-grid);
+    } else {
+        tp = t;
+        ta = t;
+    }
+}
+
 // Nodes x_i (in t^2) and weights w_i (sum w_i = F_0(T)) of the n-point Rys rule.
 __device__ __forceinline__ void rys_eval(const RysTable& tab, int n, double T, double* x, double* w) {
     if (T >= tab.tmax) {

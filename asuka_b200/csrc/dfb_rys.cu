@@ -187,8 +187,8 @@ __global__ void __launch_bounds__(DFB_WARPS_PER_BLOCK * 32)
         const long tl = unit / nchunk;
         const int ch = (int)(unit - tl * nchunk);
         const long task = t0 + tl;
-        const long tp = naux_grid > 0 ? task / naux_grid : task;
-        const long ta = naux_grid > 0 ? task - tp * naux_grid : task;
+        long tp, ta;
+        task_indices(task, naux_grid, tp, ta);
         const int pair = task_pair[tp];
         const int C = task_aux[ta];
         const int shA = ps.shA[pair];
@@ -336,8 +336,8 @@ __global__ void __launch_bounds__(DFB_WARPS_PER_BLOCK * 32)
         const int i0 = (int)(unit - tl * nec) * DFB_EPI_CHUNK;
         const int i1 = (i0 + DFB_EPI_CHUNK < ntile) ? i0 + DFB_EPI_CHUNK : ntile;
         const long task = t0 + tl;
-        const long tp = naux_grid > 0 ? task / naux_grid : task;
-        const long ta = naux_grid > 0 ? task - tp * naux_grid : task;
+        long tp, ta;
+        task_indices(task, naux_grid, tp, ta);
         const int pair = task_pair[tp];
         const int C = task_aux[ta];
         const int shA = ps.shA[pair];

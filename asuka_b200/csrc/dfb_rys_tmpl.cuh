@@ -419,8 +419,8 @@ __device__ __forceinline__ void rys_thread_body(const TmplArgs& g, long task, do
     // per-thread root slot after the optional gradient buffer
     extern __shared__ double smem_all[];
     double* sroot = smem_all + ((CL::DERIV && g.smem_grad) ? g.natm * 3 : 0) + threadIdx.x * (2 * NR);
-    const long tp = g.naux_grid > 0 ? task / g.naux_grid : task;
-    const long ta = g.naux_grid > 0 ? task - tp * g.naux_grid : task;
+    long tp, ta;
+    task_indices(task, g.naux_grid, tp, ta);
     const int pair = g.task_pair[tp];
     const int C = g.task_aux[ta];
     const int shA = g.ps.shA[pair];
@@ -516,12 +516,23 @@ __device__ __forceinline__ void rys_thread_body(const TmplArgs& g, long task, do
         const int atB = g.ps.b_dummy ? -1 : g.ps.atom[shB];
         const int atC = g.ax.atom[C];
         double* G = g.smem_grad ? sgrad : g.grad;
+        // With the aux-major task grid the lanes of a warp usually share the aux
+        // shell, hence atom C: when all 32 lanes are converged and agree, reduce
+        // over the warp first instead of 32 atomics on one address.
+        const unsigned act = __activemask();
+        const bool uniformC = (act == 0xffffffffu) && __all_sync(0xffffffffu, atC == __shfl_sync(0xffffffffu, atC, 0));
 #pragma unroll
         for (int d = 0; d < 3; ++d) {
             const double vA = fac * gA[d], vB = fac * gB[d];
             if (CL::MODE != 3) atomicAdd(G + 3 * atA + d, vA);
             if (CL::MODE != 2 && atB >= 0) atomicAdd(G + 3 * atB + d, vB);
-            atomicAdd(G + 3 * atC + d, -(vA + vB));
+            double vC = -(vA + vB);
+            if (uniformC) {
+                for (int s = 16; s > 0; s >>= 1) vC += __shfl_xor_sync(0xffffffffu, vC, s);
+                if ((threadIdx.x & 31) == 0) atomicAdd(G + 3 * atC + d, vC);
+            } else {
+                atomicAdd(G + 3 * atC + d, vC);
+            }
         }
     }
 }

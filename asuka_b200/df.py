@@ -250,6 +250,9 @@ class DFEngine:
                 sel = np.nonzero((la == a) & (lb == b) & live)[0]
                 if sel.size == 0:
                     continue
+                # pairs by decreasing primitive-pair count: with the aux-major task
+                # grid a warp walks pairs of similar cost against one aux shell
+                sel = sel[np.argsort(-cnt[sel], kind="stable")]
                 pairs = i32(sel)
                 for c, auxs in self.aux_by_l.items():
                     self.classes3c.append((int(a), int(b), int(c), pairs, auxs))
@@ -428,7 +431,7 @@ class DFEngine:
             X.zero_()
         self._slices_int = self._scratch_slices(False)
         self._fanout([self._launch_int(la, lb, lc, self.ps_ao, self.axs, pairs, auxs, pairs.numel() * auxs.numel(),
-                                       auxs.numel(), 0, X, s) for la, lb, lc, pairs, auxs in self.classes3c])
+                                       -pairs.numel(), 0, X, s) for la, lb, lc, pairs, auxs in self.classes3c])
         return X
 
     def deriv3c(self, bar: torch.Tensor, grad: torch.Tensor, layout: str = "Qmn") -> torch.Tensor:
@@ -443,7 +446,7 @@ class DFEngine:
         bar = bar.contiguous()
         self._slices_der = self._scratch_slices(True)
         self._fanout([self._launch_deriv(la, lb, lc, self.ps_ao, self.axs, pairs, auxs, pairs.numel() * auxs.numel(),
-                                         auxs.numel(), 0, bar, s, grad) for la, lb, lc, pairs, auxs in self.classes3c])
+                                         -pairs.numel(), 0, bar, s, grad) for la, lb, lc, pairs, auxs in self.classes3c])
         return grad
 
     def deriv2c(self, bar: torch.Tensor, grad: torch.Tensor) -> torch.Tensor:

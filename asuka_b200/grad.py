@@ -38,7 +38,11 @@ def _mm(A, B, precision):
 
 
 def df_forward(engine: DFEngine, Cw: torch.Tensor, precision: str = "fp64", X: torch.Tensor | None = None):
-    """Integrals at the engine's current geometry, then (E_2e, J, K) and the saved intermediates."""
+    """Integrals at the engine's current geometry, then (E_2e, J, K) and the saved intermediates.
+
+    With D = Cw Cw^T the Coulomb density rho_P = <X_P, D> = sum Cw * (X_P Cw) is read
+    from Y = X Cw (needed for K anyway) instead of a second pass over X.
+    """
     nao, naux = engine.nao, engine.naux
     nocc = Cw.shape[1]
     V = engine.metric()
@@ -47,14 +51,19 @@ def df_forward(engine: DFEngine, Cw: torch.Tensor, precision: str = "fp64", X: t
     X2 = X.view(naux, nao * nao)
     D = Cw @ Cw.T
     D = 0.5 * (D + D.T)
-    rho = X2 @ D.reshape(-1)
+    Y = (X.view(naux * nao, nao) @ Cw).view(naux, nao * nocc)
+    rho = Y @ Cw.reshape(-1)
     d = torch.cholesky_solve(rho.view(-1, 1), L).view(-1)
     J = (d @ X2).view(nao, nao)
     J = 0.5 * (J + J.T)
-    Y = _mm(X.view(naux * nao, nao), Cw, precision).view(naux, nao * nocc)
-    W = torch.linalg.solve_triangular(L, Y, upper=False)
+    if precision == "fp64":
+        W = torch.linalg.solve_triangular(L, Y, upper=False)
+    else:
+        # mixed: the compute-bound solve as a split-BF16 GEMM with L^-1
+        Linv = torch.linalg.solve_triangular(L, torch.eye(naux, dtype=L.dtype, device=L.device), upper=False)
+        W = _mixed.matmul(Linv, Y, kblock=4096)
     W2 = W.view(naux, nao, nocc).permute(1, 0, 2).reshape(nao, naux * nocc)
-    K = _mm(W2, W2.T.contiguous(), precision) if precision != "fp64" else W2 @ W2.T
+    K = _mixed.syrk(W2) if precision != "fp64" else W2 @ W2.T
     K = 0.5 * (K + K.T)
     E = 0.5 * torch.dot(rho, d) - 0.25 * torch.sum(D * K)
     return E, J, K, dict(X=X, L=L, d=d, W=W, D=D)
@@ -71,11 +80,12 @@ def df_backward(engine: DFEngine, Cw: torch.Tensor, saved: dict, grad: torch.Ten
     M = 0.5 * (M + M.transpose(1, 2))
     Z = torch.linalg.solve_triangular(L.T, M.reshape(naux, nocc * nocc), upper=True)
     Zq = Z.view(naux, nocc, nocc)
-    # Gamma_P = d_P D - 1/2 Cw Z_P Cw^T, written over X's storage (X is not needed afterwards)
+    # Gamma_P = d_P D - 1/2 Cw Z_P Cw^T = Cw (d_P I - 1/2 Z_P) Cw^T since D = Cw Cw^T:
+    # one batched GEMM, written over X's storage (X is not needed afterwards)
+    Zp = -0.5 * Zq + d.view(naux, 1, 1) * torch.eye(nocc, dtype=Zq.dtype, device=Zq.device)
+    T = torch.matmul(Zp, Cw.T)  # (naux, nocc, nao)
     G3 = X
-    T = torch.matmul(Zq, Cw.T)  # (naux, nocc, nao)
     torch.matmul(Cw, T, out=G3)
-    G3.mul_(-0.5).add_(d.view(naux, 1, 1) * D.view(1, nao, nao))
     G2 = -0.5 * torch.outer(d, d) + 0.25 * (Z @ Z.T)
     if grad is None:
         grad = torch.zeros((engine.natm, 3), dtype=torch.float64, device=X.device)

@@ -11,10 +11,11 @@ callee and returned fully symmetric, as the reference's workspace does.
 Precision modes:
 
 * ``'fp64'``  -- FP64 GEMMs (cuBLAS DGEMM through torch);
-* ``'mixed'`` -- the exchange half-transform and rank-k update run as
-  split-BF16 products (each FP64 operand split into three BF16 terms, the six
-  leading cross products accumulated in FP32 per block and summed in FP64),
-  see ``asuka_b200.mixed``.  J stays an FP64 GEMV (it is HBM-bound).
+* ``'mixed'`` -- the exchange rank-k update K = U U^T (the compute-bound
+  step) runs as split-BF16 products (each FP64 operand split into three BF16
+  terms, the leading cross products accumulated in FP32 per block and summed
+  in FP64), see ``asuka_b200.mixed``.  The half-transform U = B Cw and J are
+  HBM-bound (one pass over B) and stay FP64.
 """
 
 from __future__ import annotations
@@ -49,9 +50,9 @@ def df_K_from_BQ_Cw(BQ: torch.Tensor, Cw: torch.Tensor, q_block: int = 256, prec
             U2 = U.permute(1, 0, 2).reshape(nao, -1)
             K += U2 @ U2.T
         else:
-            U = _mixed.matmul(blk.reshape(-1, nao), Cw).reshape(q1 - q0, nao, nocc)
+            U = torch.matmul(blk.reshape(-1, nao), Cw).reshape(q1 - q0, nao, nocc)
             U2 = U.permute(1, 0, 2).reshape(nao, -1)
-            K += _mixed.matmul(U2, U2.T.contiguous())
+            K += _mixed.syrk(U2)
     return _sym(K)
 
 

@@ -44,3 +44,17 @@ def matmul(A: torch.Tensor, B: torch.Tensor, kblock: int = KBLOCK) -> torch.Tens
         acc += _mm32(a0, b2) + _mm32(a1, b1) + _mm32(a2, b0)
         out += acc
     return out
+
+
+def syrk(A: torch.Tensor, kblock: int = 16384) -> torch.Tensor:
+    """A @ A^T for FP64 A (m, k) via split-BF16: per k block A is split once into
+    A0 + A1 + A2 and the symmetric product keeps A0A0^T + (A0A1^T + A0A2^T) + sym + A1A1^T
+    -- four BF16 GEMMs with FP32 accumulation -- summed in FP64."""
+    m, k = A.shape
+    out = torch.zeros((m, m), dtype=torch.float64, device=A.device)
+    for k0 in range(0, k, kblock):
+        k1 = min(k, k0 + kblock)
+        a0, a1, a2 = split3(A[:, k0:k1])
+        cross = (_mm32(a0, a1.T) + _mm32(a0, a2.T)).to(torch.float64)
+        out += _mm32(a0, a0.T).to(torch.float64) + _mm32(a1, a1.T).to(torch.float64) + cross + cross.T
+    return out

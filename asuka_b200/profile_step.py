@@ -82,17 +82,21 @@ def df_forward_from_X(eng, Cw, precision, X, L, mark=lambda k: None):
     nocc = Cw.shape[1]
     X2 = X.view(naux, nao * nao)
     D = Cw @ Cw.T
-    rho = X2 @ D.reshape(-1)
+    mm = (lambda A, B: A @ B) if precision == "fp64" else _mixed.matmul
+    Y = (X.view(naux * nao, nao) @ Cw).view(naux, nao * nocc)
+    mark("jk_Y")
+    rho = Y @ Cw.reshape(-1)
     d = torch.cholesky_solve(rho.view(-1, 1), L).view(-1)
     J = (d @ X2).view(nao, nao)
     mark("jk_rho_J")
-    mm = (lambda A, B: A @ B) if precision == "fp64" else _mixed.matmul
-    Y = mm(X.view(naux * nao, nao), Cw).view(naux, nao * nocc)
-    mark("jk_Y")
-    W = torch.linalg.solve_triangular(L, Y, upper=False)
+    if precision == "fp64":
+        W = torch.linalg.solve_triangular(L, Y, upper=False)
+    else:
+        Linv = torch.linalg.solve_triangular(L, torch.eye(naux, dtype=L.dtype, device=L.device), upper=False)
+        W = _mixed.matmul(Linv, Y, kblock=4096)
     mark("jk_W_trsm")
     W2 = W.view(naux, nao, nocc).permute(1, 0, 2).reshape(nao, naux * nocc)
-    K = mm(W2, W2.T.contiguous())
+    K = mm(W2, W2.T) if precision == "fp64" else _mixed.syrk(W2)
     E = 0.5 * torch.dot(rho, d) - 0.25 * torch.sum(D * K)
     return E, J, K, dict(X=X, L=L, d=d, W=W, D=D)
 
@@ -104,9 +108,9 @@ def adjoints(eng, Cw, saved):
     M = torch.matmul(Cw.T, W.view(naux, nao, nocc))
     M = 0.5 * (M + M.transpose(1, 2))
     Z = torch.linalg.solve_triangular(L.T, M.reshape(naux, nocc * nocc), upper=True)
-    T = torch.matmul(Z.view(naux, nocc, nocc), Cw.T)
+    Zp = -0.5 * Z.view(naux, nocc, nocc) + d.view(naux, 1, 1) * torch.eye(nocc, dtype=Z.dtype, device=Z.device)
+    T = torch.matmul(Zp, Cw.T)
     torch.matmul(Cw, T, out=X)
-    X.mul_(-0.5).add_(d.view(naux, 1, 1) * D.view(1, nao, nao))
     G2 = -0.5 * torch.outer(d, d) + 0.25 * (Z @ Z.T)
     return X, G2
 

@@ -83,8 +83,9 @@ int dfb_pair_tables(const double *cxyz, const int *shell_pstart, const int *shel
 /*
  * Rys integrals for one angular class (la, lb, lc) over ntask tasks, written
  * straight into the output.  Tasks are (task_pair[t], task_aux[t]) when
- * naux_grid == 0, or the grid (task_pair[t / naux_grid], task_aux[t % naux_grid])
- * when naux_grid > 0 (ntask = npairs * naux_grid).  Output (the
+ * naux_grid == 0, the pair-major grid (task_pair[t / naux_grid], task_aux[t %
+ * naux_grid]) when naux_grid > 0 (ntask = npairs * naux_grid), or the aux-major
+ * grid (task_pair[t % n], task_aux[t / n]), n = -naux_grid, when naux_grid < 0.  Output (the
  * reference's tile kernel plus scatter, K3+K7, in one pass):
  *   mode 0: 3c, out[(P0+c)*sP + mu*sM + nu*sN] and the (nu, mu) mirror;
  *   mode 1: metric, out[(Q0+c)*sP + (P0+a)*sM] and out[(P0+a)*sP + (Q0+c)*sM].
