@@ -343,26 +343,50 @@ class DFEngine:
         self._aux_blocks, self._aux_blocks_n = blocks, max_naux
         return blocks
 
-    def int3c_block(self, blk, p0: int, p1: int, out: torch.Tensor | None = None) -> torch.Tensor:
-        """X rows for one aux block as (p1-p0, nao, nao) (streamed DF, ``gpu.py:2742``)."""
+    def int3c_block(self, blk, p0: int, p1: int, out: torch.Tensor | None = None,
+                    dropped_zero: bool = False) -> torch.Tensor:
+        """X rows for one aux block as (p1-p0, nao, nao) (streamed DF, ``gpu.py:2742``).
+
+        Entries of screened-out shell pairs are not written; they are zeroed here
+        unless ``dropped_zero`` says the buffer already holds zeros there (the set
+        of dropped pairs is the same for every block, so a reused buffer needs
+        zeroing once).
+        """
         axb, _shifted, byl = blk
         nao = self.nao
         X = out if out is not None else torch.empty((p1 - p0, nao, nao), dtype=torch.float64, device=self.device)
-        if self.n_dropped_pairs:
+        if self.n_dropped_pairs and not dropped_zero:
             X.zero_()
-        scr = self._scratch_for(False)
-        L = _lib.lib()
+        self._slices_int = self._scratch_slices(False)
+        launches = []
         seen = set()
         for la, lb, lc, pairs, _auxs in self.classes3c:
             if lc not in byl or (la, lb, lc) in seen:
                 continue
             seen.add((la, lb, lc))
             auxs = byl[lc]
-            rc = L.dfb_rys_int(la, lb, lc, ctypes.byref(self.ps_ao), ctypes.byref(axb), _lib.ptr(pairs),
-                               _lib.ptr(auxs), pairs.numel() * auxs.numel(), auxs.numel(), 0, _lib.ptr(X),
-                               nao * nao, nao, 1, _lib.ptr(scr), scr.numel(), _stream())
-            _lib.check(rc, f"dfb_rys_int 3c block ({la},{lb},{lc})")
+            launches.append(self._launch_int(la, lb, lc, self.ps_ao, axb, pairs, auxs, pairs.numel() * auxs.numel(),
+                                             -pairs.numel(), 0, X, (nao * nao, nao, 1)))
+        self._fanout(launches)
         return X
+
+    def deriv3c_block(self, blk, bar: torch.Tensor, grad: torch.Tensor) -> torch.Tensor:
+        """grad += sum over one aux block of bar[P-p0, mu, nu] d(mu nu|P)/dR (block-local adjoint)."""
+        axb, _shifted, byl = blk
+        nao = self.nao
+        bar = bar.contiguous()
+        self._slices_der = self._scratch_slices(True)
+        launches = []
+        seen = set()
+        for la, lb, lc, pairs, _auxs in self.classes3c:
+            if lc not in byl or (la, lb, lc) in seen:
+                continue
+            seen.add((la, lb, lc))
+            auxs = byl[lc]
+            launches.append(self._launch_deriv(la, lb, lc, self.ps_ao, axb, pairs, auxs, pairs.numel() * auxs.numel(),
+                                               -pairs.numel(), 0, bar, (nao * nao, nao, 1), grad))
+        self._fanout(launches)
+        return grad
 
     def _scratch_slices(self, deriv: bool):
         """Scratch for the generic kernels: one slice per side stream (launches overlap)."""

@@ -122,6 +122,109 @@ def df_energy(coords: torch.Tensor, Cw: torch.Tensor, engine: DFEngine, precisio
     return DFEnergyFunction.apply(coords, Cw, engine, precision)
 
 
+# ---------------------------------------------------------------- streamed (B never stored)
+
+def _solve_lower_inplace(L: torch.Tensor, Y: torch.Tensor, precision: str, ncol: int = 1 << 18) -> torch.Tensor:
+    """Y <- L^-1 Y in place, by column blocks (one block copy alive at a time).
+
+    FP64: triangular solves.  Mixed: L^-1 formed once in FP64, split once into
+    BF16 terms, and applied to each column block as a split-BF16 GEMM.
+    """
+    n, m = Y.shape
+    ncol = max(1, min(m, ncol * 1024 // max(n, 1)))
+    if precision == "fp64":
+        for c0 in range(0, m, ncol):
+            c1 = min(m, c0 + ncol)
+            Y[:, c0:c1] = torch.linalg.solve_triangular(L, Y[:, c0:c1].contiguous(), upper=False)
+        return Y
+    Linv = torch.linalg.solve_triangular(L, torch.eye(n, dtype=L.dtype, device=L.device), upper=False)
+    sp = _mixed.split3(Linv)
+    del Linv
+    for c0 in range(0, m, ncol):
+        c1 = min(m, c0 + ncol)
+        Y[:, c0:c1] = _mixed.matmul(None, Y[:, c0:c1].contiguous(), kblock=4096, a_split=sp)
+    return Y
+
+
+def df_energy_grad_streamed(engine: DFEngine, Cw: torch.Tensor, aux_block: int = 128, precision: str = "fp64",
+                            stats: dict | None = None):
+    """E_2e and dE_2e/dR without storing the 3c tensor: the integrals are recomputed per aux block.
+
+    Forward: for each aux block b, X_b -> Y_b = X_b Cw (rho from Y); then d = V^-1 rho,
+    W = L^-1 Y (in place), K = sum_Q W_Q W_Q^T by aux chunks.  Backward: M = Cw^T W,
+    Z = L^-T M, and for each block Gamma_b = Cw (d_b I - 1/2 Z_b) Cw^T contracted with the
+    block's derivative integrals (the streamed analogue of
+    ``asuka/hf/df_jk_streamed.py:167-325``, with the gradient recomputing the integrals
+    instead of reading a stored B).  The largest buffer is Y/W (naux x nao x nocc)
+    instead of the 3c tensor (naux x nao^2).  ``precision='mixed'`` runs the solve
+    W = L^-1 Y and the exchange update K as split-BF16 GEMMs (FP32 accumulation);
+    the integrals, the half-transforms and the adjoint stay FP64.
+    Returns (E, grad (natm, 3), K).
+    """
+    nao, naux = engine.nao, engine.naux
+    nocc = Cw.shape[1]
+    dev = engine.device
+    torch.cuda.reset_peak_memory_stats(dev)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(6)]
+    ev[0].record()
+    V = engine.metric()
+    L = cholesky_metric(V)
+    del V
+    blocks = engine.aux_blocks(aux_block)
+    Y = torch.empty((naux, nao * nocc), dtype=torch.float64, device=dev)
+    bmax = max(p1 - p0 for p0, p1, _ in blocks)
+    Xb_buf = torch.zeros((bmax, nao, nao), dtype=torch.float64, device=dev)
+    for p0, p1, blk in blocks:
+        Xb = engine.int3c_block(blk, p0, p1, out=Xb_buf[: p1 - p0], dropped_zero=True)
+        torch.matmul(Xb.view(-1, nao), Cw, out=Y[p0:p1].view(-1, nocc))
+    ev[1].record()
+    rho = Y @ Cw.reshape(-1)
+    d = torch.cholesky_solve(rho.view(-1, 1), L).view(-1)
+    W = _solve_lower_inplace(L, Y, precision)
+    W3 = W.view(naux, nao, nocc)
+    K = torch.zeros((nao, nao), dtype=torch.float64, device=dev)
+    qb = max(1, (1 << 27) // max(nao * nocc, 1))
+    for q0 in range(0, naux, qb):
+        Wc = W3[q0:q0 + qb].permute(1, 0, 2).reshape(nao, -1)
+        if precision == "fp64":
+            K.addmm_(Wc, Wc.T)
+        else:
+            K += _mixed.syrk(Wc)
+    K = 0.5 * (K + K.T)
+    D = Cw @ Cw.T
+    E = 0.5 * torch.dot(rho, d) - 0.25 * torch.sum(D * K)
+    ev[2].record()
+    M = torch.matmul(Cw.T, W3)
+    del W, W3, Y
+    for q0 in range(0, naux, qb):
+        Mc = M[q0:q0 + qb]
+        Mc.copy_(0.5 * (Mc + Mc.transpose(1, 2)))
+    Z = torch.linalg.solve_triangular(L.T, M.view(naux, nocc * nocc), upper=True)
+    del M
+    Zq = Z.view(naux, nocc, nocc)
+    grad = torch.zeros((engine.natm, 3), dtype=torch.float64, device=dev)
+    eye = torch.eye(nocc, dtype=Cw.dtype, device=dev)
+    ev[3].record()
+    for p0, p1, blk in blocks:
+        Zp = -0.5 * Zq[p0:p1] + d[p0:p1].view(-1, 1, 1) * eye
+        T = torch.matmul(Zp, Cw.T)
+        G3 = Xb_buf[: p1 - p0]
+        torch.matmul(Cw, T, out=G3)
+        engine.deriv3c_block(blk, G3, grad)
+    ev[4].record()
+    G2 = -0.5 * torch.outer(d, d) + 0.25 * (Z @ Z.T)
+    engine.deriv2c(G2, grad)
+    ev[5].record()
+    if stats is not None:
+        torch.cuda.synchronize(dev)
+        stats.update(peak_hbm_bytes=int(torch.cuda.max_memory_allocated(dev)), nblocks=len(blocks),
+                     x_bytes_if_stored=int(naux) * nao * nao * 8, y_bytes=int(naux) * nao * nocc * 8,
+                     ms_int3c_and_Y=ev[0].elapsed_time(ev[1]), ms_jk=ev[1].elapsed_time(ev[2]),
+                     ms_adjoint=ev[2].elapsed_time(ev[3]), ms_deriv3c=ev[3].elapsed_time(ev[4]),
+                     ms_deriv2c=ev[4].elapsed_time(ev[5]), ms_total=ev[0].elapsed_time(ev[5]))
+    return E, grad, K
+
+
 # ---------------------------------------------------------------- reference seam
 
 def compute_df_gradient_contributions_analytic_packed_bases(ao_basis, aux_basis, *, atom_coords_bohr, B_ao,

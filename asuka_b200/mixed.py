@@ -30,14 +30,22 @@ def _mm32(a: torch.Tensor, b: torch.Tensor) -> torch.Tensor:
     return torch.mm(a, b, out_dtype=torch.float32)
 
 
-def matmul(A: torch.Tensor, B: torch.Tensor, kblock: int = KBLOCK) -> torch.Tensor:
-    """A @ B for FP64 A (m, k), B (k, n) via six split-BF16 products; FP64 result."""
-    m, k = A.shape
+def matmul(A: torch.Tensor | None, B: torch.Tensor, kblock: int = KBLOCK,
+           a_split: tuple[torch.Tensor, torch.Tensor, torch.Tensor] | None = None) -> torch.Tensor:
+    """A @ B for FP64 A (m, k), B (k, n) via six split-BF16 products; FP64 result.
+
+    ``a_split`` = split3(A) computed once by the caller replaces A when the same
+    left operand multiplies many right-hand blocks.
+    """
+    m, k = A.shape if a_split is None else a_split[0].shape
     n = B.shape[1]
-    out = torch.zeros((m, n), dtype=torch.float64, device=A.device)
+    out = torch.zeros((m, n), dtype=torch.float64, device=B.device)
     for k0 in range(0, k, kblock):
         k1 = min(k, k0 + kblock)
-        a0, a1, a2 = split3(A[:, k0:k1])
+        if a_split is None:
+            a0, a1, a2 = split3(A[:, k0:k1])
+        else:
+            a0, a1, a2 = (t[:, k0:k1] for t in a_split)
         b0, b1, b2 = split3(B[k0:k1])
         acc = _mm32(a0, b0).to(torch.float64)
         acc += _mm32(a0, b1) + _mm32(a1, b0)

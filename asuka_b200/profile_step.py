@@ -25,6 +25,8 @@ WORKLOADS = {
     "decane": lambda: geo.decane(0, "ma-svp"),
     "n2": lambda: geo.n2("ma-svp"),
     "w1": lambda: geo.water("ma-tzvp"),
+    "w32": lambda: geo.water_cluster(32, 0, "ma-tzvp"),
+    "w64": lambda: geo.water_cluster(64, 0, "ma-tzvp"),
 }
 
 
@@ -168,8 +170,21 @@ def main():
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--only", default=None, choices=[None, "int3c", "deriv3c", "metric", "deriv2c", "step"])
     ap.add_argument("--classes", action="store_true", help="time every angular class of int3c and deriv3c")
+    ap.add_argument("--streamed", type=int, default=0, metavar="NAUX_BLOCK",
+                    help="streamed energy+gradient (3c recomputed per aux block of this size); prints peak HBM")
     args = ap.parse_args()
     mol, eng, Cw, R = setup(args.workload)
+    if args.streamed:
+        from .grad import df_energy_grad_streamed
+
+        for i in range(max(1, args.steps)):
+            st = {}
+            E, g, _ = df_energy_grad_streamed(eng, Cw, aux_block=args.streamed, precision=args.precision, stats=st)
+            print(json.dumps({"workload": args.workload, "nao": eng.nao, "naux": eng.naux, "nocc": Cw.shape[1],
+                              "precision": args.precision, "run": i, "E2": float(E),
+                              "grad_norm": float(g.norm()), "n_dropped_pairs": int(eng.n_dropped_pairs),
+                              **{k: (round(v, 3) if isinstance(v, float) else v) for k, v in st.items()}}))
+        return
     if args.classes:
         print(json.dumps(class_times(eng, mol)))
         return

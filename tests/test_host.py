@@ -59,3 +59,17 @@ def test_nuclear_repulsion_gradient_matches_finite_difference():
             R[a, c] -= 2 * h
             em = mol.with_coords(R).energy_nuc()
             assert abs((ep - em) / (2 * h) - g[a, c]) < 1e-7
+
+
+def test_engine_methods_called_are_defined():
+    """Every ``self.<name>(`` call in the engine names an attribute the class defines
+    (the GPU-only methods cannot be exercised here)."""
+    import re
+
+    from asuka_b200 import df
+
+    src = open(df.__file__).read()
+    called = set(re.findall(r"self\.(_?[a-zA-Z]\w*)\(", src))
+    assigned = set(re.findall(r"self\.(\w+)\s*=", src))
+    missing = sorted(n for n in called if not hasattr(df.DFEngine, n) and n not in assigned)
+    assert not missing, missing
