@@ -38,6 +38,21 @@ _TABLE_READY: set[int] = set()
 PRIM_SCREEN = 1e-20  # primitive-pair magnitude bound below which a pair is skipped (0 = evaluate all)
 NSTREAMS = int(os.environ.get("DFB_STREAMS", "4"))  # side streams for per-class launches
 NROOTS_SLOTS = 11  # DFB_NROOTS_MAX + 1
+_SIDE_STREAMS: dict[int, list] = {}
+
+
+class ScratchHolder:
+    """Device scratch for the generic kernels, shared by engines that run one after another
+    on the same streams (a batch of molecules): one buffer, grown to the largest need."""
+
+    def __init__(self):
+        self.t: torch.Tensor | None = None
+
+    def get(self, need: int, device) -> torch.Tensor:
+        if self.t is None or self.t.numel() < need:
+            self.t = None
+            self.t = torch.empty(need, dtype=torch.float64, device=device)
+        return self.t[:need]
 
 
 @functools.lru_cache(maxsize=1)
@@ -87,7 +102,7 @@ class DFEngine:
     """Device-side state of the DF Rys integrals for one (AO, aux) basis pair."""
 
     def __init__(self, ao_basis, aux_basis, device=None, atom_coords_bohr: np.ndarray | None = None,
-                 prim_screen: float = PRIM_SCREEN):
+                 prim_screen: float = PRIM_SCREEN, scratch: ScratchHolder | None = None):
         self.device = torch.device(device) if device is not None else torch.device("cuda", torch.cuda.current_device())
         if self.device.type != "cuda":
             raise RuntimeError("DFEngine runs on CUDA devices only (no CPU fallback)")
@@ -159,7 +174,7 @@ class DFEngine:
                 sel = np.nonzero((lP == a) & (lQ == c))[0]
                 if sel.size:
                     self.classes2c.append((int(a), int(c), i32(P[sel]), i32(Q[sel])))
-        self._scratch = None
+        self._scratch = scratch if scratch is not None else ScratchHolder()
         self._build_ao_pairs(ao.shell_cxyz)
         self._build_pair_tables()
 
@@ -167,9 +182,10 @@ class DFEngine:
     def _streams(self):
         """Side streams for class launches: classes write disjoint outputs (or add to the
         gradient atomically), so their kernels may overlap and fill each other's tails."""
-        if getattr(self, "_side", None) is None:
-            self._side = [torch.cuda.Stream(device=self.device) for _ in range(NSTREAMS)]
-        return self._side
+        idx = self.device.index if self.device.index is not None else torch.cuda.current_device()
+        if idx not in _SIDE_STREAMS:
+            _SIDE_STREAMS[idx] = [torch.cuda.Stream(device=self.device) for _ in range(NSTREAMS)]
+        return _SIDE_STREAMS[idx]
 
     def _fanout(self, launches):
         """Run launch(stream_ptr) callables round-robin over side streams, ordered after and
@@ -294,10 +310,7 @@ class DFEngine:
         key = (deriv, os.environ.get("DFB_DISABLE_TMPL"), id(self.classes3c))
         cache = self.__dict__.setdefault("_need_cache", {})
         if key in cache:
-            need = cache[key] * copies
-            if self._scratch is None or self._scratch.numel() < need:
-                self._scratch = torch.empty(need, dtype=torch.float64, device=self.device)
-            return self._scratch[:need]
+            return self._scratch.get(cache[key] * copies, self.device)
         L = _lib.lib()
         need = 1
         for la, lb, lc, pairs, auxs in self.classes3c:
@@ -309,10 +322,7 @@ class DFEngine:
             _lib.check(0 if n >= 0 else int(n), "dfb_rys_scratch_doubles")
             need = max(need, n)
         cache[key] = need
-        need *= copies
-        if self._scratch is None or self._scratch.numel() < need:
-            self._scratch = torch.empty(need, dtype=torch.float64, device=self.device)
-        return self._scratch[:need]
+        return self._scratch.get(need * copies, self.device)
 
     def aux_blocks(self, max_naux: int = 256):
         """Contiguous aux-shell blocks of at most ``max_naux`` functions, aligned to shells
