@@ -149,8 +149,11 @@ __device__ __forceinline__ void build_G(double* G, int nmax, int mmax, double g0
 // U | WA | WB (derivative; flushed once per AO primitive pair).  Splitting the
 // elements of a task over warps keeps the SMs busy for the heavy high-l classes,
 // which have few tasks.
+#ifndef DFB_ACC_MIN_BLOCKS
+#define DFB_ACC_MIN_BLOCKS 3  // resident blocks per SM the accumulation kernel is compiled for
+#endif
 template <int KB, bool DERIV>
-__global__ void __launch_bounds__(DFB_WARPS_PER_BLOCK * 32)
+__global__ void __launch_bounds__(DFB_WARPS_PER_BLOCK * 32, DFB_ACC_MIN_BLOCKS)
     k_rys_acc(ClassInfo ci, dfb_pair_side_t ps, dfb_aux_side_t ax, const int* __restrict__ task_pair,
               const int* __restrict__ task_aux, long t0, long nt, long naux_grid, double* __restrict__ scratch,
               long slot, RysTable tab) {
@@ -165,18 +168,23 @@ __global__ void __launch_bounds__(DFB_WARPS_PER_BLOCK * 32)
     const int chunk_elems = 32 * KB;
     const int nchunk = (ci.nef + chunk_elems - 1) / chunk_elems;
     const int M = ci.mmax + 1;
-    int off[KB];
+    // per element of the lane: offsets of its x, y and z factors inside one root's
+    // three tables (y and z include the table stride); elements past the end read
+    // entry 0 and are never stored
+    int ox[KB], oy[KB], oz[KB];
     auto make_offsets = [&](int cbase) {
 #pragma unroll
         for (int k = 0; k < KB; ++k) {
             const int t = cbase + lane + 32 * k;
-            off[k] = -1;
+            ox[k] = oy[k] = oz[k] = 0;
             if (t < ci.nef) {
                 const int e = t / ci.nf, f = t - (t / ci.nf) * ci.nf;
                 int ex, ey, ez, fx, fy, fz;
                 decode_e(ci, e, ex, ey, ez);
                 decode_cart(ci.lc, f, fx, fy, fz);
-                off[k] = (ex * M + fx) | ((ey * M + fy) << 10) | ((ez * M + fz) << 20);
+                ox[k] = ex * M + fx;
+                oy[k] = ci.gt + ey * M + fy;
+                oz[k] = 2 * ci.gt + ez * M + fz;
             }
         }
     };
@@ -210,8 +218,8 @@ __global__ void __launch_bounds__(DFB_WARPS_PER_BLOCK * 32)
 #pragma unroll
         for (int k = 0; k < KB; ++k) {
             acc[k] = 0.0;
-            if (DERIV && off[k] >= 0) {
-                const int t = cbase + lane + 32 * k;
+            const int t = cbase + lane + 32 * k;
+            if (DERIV && t < ci.nef) {
                 E[t] = 0.0;
                 E[ci.nef + t] = 0.0;
                 E[2 * ci.nef + t] = 0.0;
@@ -240,12 +248,9 @@ __global__ void __launch_bounds__(DFB_WARPS_PER_BLOCK * 32)
                 }
                 const double T = p * q * inv * PQ2;
                 const double pref = kTwoPi52 / (p * q * sqrt(p + q)) * ps.cK[p0 + iab] * ax.pcoef[c0 + ic];
-                double xr[DFB_NROOTS_MAX], wr[DFB_NROOTS_MAX];
-                rys_eval(tab, ci.nr, T, xr, wr);
-                for (int u = 0; u < ci.nr; ++u) {
-                    it[8 + u] = xr[u];
-                    it[8 + ci.nr + u] = pref * wr[u];
-                }
+                // nodes and weights straight into the lane's shared-memory record
+                rys_eval(tab, ci.nr, T, it + 8, it + 8 + ci.nr);
+                for (int u = 0; u < ci.nr; ++u) it[8 + ci.nr + u] *= pref;
             }
             __syncwarp();
             const int nb = (int)((nitems - base) < 32 ? (nitems - base) : 32);
@@ -265,17 +270,11 @@ __global__ void __launch_bounds__(DFB_WARPS_PER_BLOCK * 32)
                     build_G(gtab + (u * 3 + d) * ci.gt, ci.nmax, ci.mmax, g00, Cd, Cpd, B0, B1, B1p);
                 }
                 __syncwarp();
+                // roots outer, elements inner: KB independent FMA chains per root
+                const double* g = gtab;
+                for (int u = 0; u < ci.nr; ++u, g += 3 * ci.gt) {
 #pragma unroll
-                for (int k = 0; k < KB; ++k) {
-                    if (off[k] >= 0) {
-                        const int ox = off[k] & 1023, oy = (off[k] >> 10) & 1023, oz = off[k] >> 20;
-                        double v = 0.0;
-                        for (int u = 0; u < ci.nr; ++u) {
-                            const double* g = gtab + u * 3 * ci.gt;
-                            v = fma(g[ox] * g[ci.gt + oy], g[2 * ci.gt + oz], v);
-                        }
-                        acc[k] += v;
-                    }
+                    for (int k = 0; k < KB; ++k) acc[k] = fma(g[ox[k]] * g[oy[k]], g[oz[k]], acc[k]);
                 }
                 if (DERIV) {
                     const long gidx = base + jj;
@@ -286,7 +285,7 @@ __global__ void __launch_bounds__(DFB_WARPS_PER_BLOCK * 32)
 #pragma unroll
                         for (int k = 0; k < KB; ++k) {
                             const int t = cbase + lane + 32 * k;
-                            if (off[k] >= 0) {
+                            if (t < ci.nef) {
                                 E[t] += acc[k];
                                 E[ci.nef + t] += a2 * acc[k];
                                 E[2 * ci.nef + t] += b2 * acc[k];
@@ -301,7 +300,7 @@ __global__ void __launch_bounds__(DFB_WARPS_PER_BLOCK * 32)
         if (!DERIV) {
 #pragma unroll
             for (int k = 0; k < KB; ++k) {
-                if (off[k] >= 0) E[cbase + lane + 32 * k] = acc[k];
+                if (cbase + lane + 32 * k < ci.nef) E[cbase + lane + 32 * k] = acc[k];
             }
         }
         __syncwarp();
@@ -380,26 +379,34 @@ __global__ void __launch_bounds__(DFB_WARPS_PER_BLOCK * 32)
                     const double* U = E;
                     const double* WA = E + ci.nef;
                     const double* WB = E + 2 * ci.nef;
-#pragma unroll
+                    // (a b|c) of WB is shared by the three directions of the B derivative
+                    const double wb0 = ps.b_dummy ? 0.0 : hrr(ci, WB, a[0], a[1], a[2], b[0], b[1], b[2], ic, AB);
+                    // one direction per iteration, not unrolled: five HRR bodies in the
+                    // code instead of fifteen keeps the kernel inside the instruction cache
+#pragma unroll 1
                     for (int d = 0; d < 3; ++d) {
-                        int ap[3] = {a[0], a[1], a[2]};
-                        ap[d] += 1;
-                        double dA = hrr(ci, WA, ap[0], ap[1], ap[2], b[0], b[1], b[2], ic, AB);
-                        if (a[d] > 0) {
-                            int am[3] = {a[0], a[1], a[2]};
-                            am[d] -= 1;
-                            dA -= (double)a[d] * hrr(ci, U, am[0], am[1], am[2], b[0], b[1], b[2], ic, AB);
-                        }
-                        gA[d] += gam * dA;
+                        const int ex = d == 0, ey = d == 1, ez = d == 2;
+                        const int ad = d == 0 ? a[0] : (d == 1 ? a[1] : a[2]);
+                        const int bd = d == 0 ? b[0] : (d == 1 ? b[1] : b[2]);
+                        const double abd = d == 0 ? AB[0] : (d == 1 ? AB[1] : AB[2]);
+                        double dA = hrr(ci, WA, a[0] + ex, a[1] + ey, a[2] + ez, b[0], b[1], b[2], ic, AB);
+                        if (ad > 0)
+                            dA -= (double)ad * hrr(ci, U, a[0] - ex, a[1] - ey, a[2] - ez, b[0], b[1], b[2], ic, AB);
+                        double dB = 0.0;
                         if (!ps.b_dummy) {
-                            double dB = hrr(ci, WB, ap[0], ap[1], ap[2], b[0], b[1], b[2], ic, AB) +
-                                        AB[d] * hrr(ci, WB, a[0], a[1], a[2], b[0], b[1], b[2], ic, AB);
-                            if (b[d] > 0) {
-                                int bm[3] = {b[0], b[1], b[2]};
-                                bm[d] -= 1;
-                                dB -= (double)b[d] * hrr(ci, U, a[0], a[1], a[2], bm[0], bm[1], bm[2], ic, AB);
-                            }
-                            gB[d] += gam * dB;
+                            dB = hrr(ci, WB, a[0] + ex, a[1] + ey, a[2] + ez, b[0], b[1], b[2], ic, AB) + abd * wb0;
+                            if (bd > 0)
+                                dB -= (double)bd * hrr(ci, U, a[0], a[1], a[2], b[0] - ex, b[1] - ey, b[2] - ez, ic, AB);
+                        }
+                        if (d == 0) {
+                            gA[0] += gam * dA;
+                            gB[0] += gam * dB;
+                        } else if (d == 1) {
+                            gA[1] += gam * dA;
+                            gB[1] += gam * dB;
+                        } else {
+                            gA[2] += gam * dA;
+                            gB[2] += gam * dB;
                         }
                     }
                 }

@@ -27,6 +27,7 @@ WORKLOADS = {
     "w1": lambda: geo.water("ma-tzvp"),
     "w32": lambda: geo.water_cluster(32, 0, "ma-tzvp"),
     "w64": lambda: geo.water_cluster(64, 0, "ma-tzvp"),
+    "w4q": lambda: geo.water_cluster(4, 0, "ma-qzvp"),
 }
 
 
@@ -170,10 +171,17 @@ def main():
     ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
     ap.add_argument("--only", default=None, choices=[None, "int3c", "deriv3c", "metric", "deriv2c", "step"])
     ap.add_argument("--classes", action="store_true", help="time every angular class of int3c and deriv3c")
+    ap.add_argument("--cls", default=None, metavar="LA,LB,LC",
+                    help="keep only this 3c angular class (with --only int3c/deriv3c or --classes)")
     ap.add_argument("--streamed", type=int, default=0, metavar="NAUX_BLOCK",
                     help="streamed energy+gradient (3c recomputed per aux block of this size); prints peak HBM")
     args = ap.parse_args()
     mol, eng, Cw, R = setup(args.workload)
+    if args.cls:
+        want = tuple(int(v) for v in args.cls.split(","))
+        eng.classes3c = [c for c in eng.classes3c if tuple(c[:3]) == want]
+        if not eng.classes3c:
+            raise SystemExit(f"class {want} does not occur in {args.workload}")
     if args.streamed:
         from .grad import df_energy_grad_streamed
 
