@@ -94,35 +94,8 @@ __device__ __forceinline__ void decode_e(const ClassInfo& ci, int e, int& x, int
 
 __constant__ int c_ncbtab[2 * DFB_LMAX + 4];  // ncart_below(L), L = 0 .. 2 LMAX + 3
 
-__device__ __forceinline__ int e_index(const ClassInfo& ci, int x, int y, int z) {
-    const int L = x + y + z;
-    return c_ncbtab[L] - c_ncbtab[ci.lmin] + cart_index(x, y, L);
-}
 
 __constant__ double c_binomtab[DFB_LMAX + 2][DFB_LMAX + 2];
-
-// (a b | f) = sum_k C(b,k) AB^(b-k) (a+k 0 | f), per direction, from E[e*nf + f].
-__device__ __forceinline__ double hrr(const ClassInfo& ci, const double* E, int ax, int ay, int az, int bx, int by,
-                                      int bz, int f, const double* AB) {
-    double sum = 0.0;
-    double px = 1.0;
-    for (int kx = bx; kx >= 0; --kx) {
-        const double cx = c_binomtab[bx][kx] * px;
-        double py = 1.0;
-        for (int ky = by; ky >= 0; --ky) {
-            const double cxy = cx * c_binomtab[by][ky] * py;
-            double pz = 1.0;
-            for (int kz = bz; kz >= 0; --kz) {
-                const double c = cxy * c_binomtab[bz][kz] * pz;
-                sum += c * E[e_index(ci, ax + kx, ay + ky, az + kz) * ci.nf + f];
-                pz *= AB[2];
-            }
-            py *= AB[1];
-        }
-        px *= AB[0];
-    }
-    return sum;
-}
 
 __device__ __forceinline__ void build_G(double* G, int nmax, int mmax, double g00, double C, double Cp, double B0,
                                         double B1, double B1p) {
@@ -308,10 +281,66 @@ __global__ void __launch_bounds__(DFB_WARPS_PER_BLOCK * 32, DFB_ACC_MIN_BLOCKS)
 }
 
 #define DFB_EPI_CHUNK 128  // tile elements per epilogue work unit
+#define DFB_HRR_TERMS 64   // capacity of one horizontal-recurrence term list (lb <= 8 needs 48)
 
-// Phase 2: one warp per (task, tile chunk) -- horizontal recurrence from the task's scratch
-// slot, then the tile goes to its final place (integrals) or is contracted with
-// the adjoint (derivative; per-block partial gradients in shared memory).
+// Terms of the horizontal recurrence for one b: (a b|f) = sum_t coef_t (a + k_t, 0|f)
+// over k_t <= b componentwise, coef_t = prod_d C(b_d, k_d) AB_d^(b_d - k_d).  The
+// lanes of a warp build the list together in the warp's shared memory.
+__device__ __forceinline__ int hrr_terms(int bx, int by, int bz, const double* AB, double* tc, int* tk, int lane) {
+    const int ny = by + 1, nz = bz + 1;
+    const int n = (bx + 1) * ny * nz;
+    for (int t = lane; t < n; t += 32) {
+        const int kx = t / (ny * nz);
+        const int r = t - kx * ny * nz;
+        const int ky = r / nz;
+        const int kz = r - ky * nz;
+        double c = c_binomtab[bx][kx] * c_binomtab[by][ky] * c_binomtab[bz][kz];
+        for (int m = kx; m < bx; ++m) c *= AB[0];
+        for (int m = ky; m < by; ++m) c *= AB[1];
+        for (int m = kz; m < bz; ++m) c *= AB[2];
+        tc[t] = c;
+        tk[t] = kx | (ky << 8) | (kz << 16);
+    }
+    return n;
+}
+
+// Position of the Cartesian component (x, y, z) in the contracted intermediate
+// (shells lmin..lmax, x-major inside a shell); ebase = -ncart_below(lmin).
+__device__ __forceinline__ int e_pos(int x, int y, int z, int ebase) {
+    const int L = x + y + z;
+    return c_ncbtab[L] + ebase + (((L - x) * (L - x + 1)) >> 1) + (L - x - y);
+}
+
+// sum_t coef_t T[(a + k_t) nf + ic] for one table, and for two tables read at the same positions.
+__device__ __forceinline__ double hrr_apply(const double* __restrict__ T, int nf, int ic, int ebase, int ax, int ay,
+                                            int az, const double* tc, const int* tk, int n) {
+    double s = 0.0;
+    for (int t = 0; t < n; ++t) {
+        const int k = tk[t];
+        const int e = e_pos(ax + (k & 255), ay + ((k >> 8) & 255), az + (k >> 16), ebase);
+        s = fma(tc[t], __ldg(T + e * nf + ic), s);
+    }
+    return s;
+}
+
+__device__ __forceinline__ void hrr_apply2(const double* __restrict__ T1, const double* __restrict__ T2, int nf, int ic,
+                                           int ebase, int ax, int ay, int az, const double* tc, const int* tk, int n,
+                                           double& s1, double& s2) {
+    s1 = s2 = 0.0;
+    for (int t = 0; t < n; ++t) {
+        const int k = tk[t];
+        const int e = e_pos(ax + (k & 255), ay + ((k >> 8) & 255), az + (k >> 16), ebase) * nf + ic;
+        s1 = fma(tc[t], __ldg(T1 + e), s1);
+        s2 = fma(tc[t], __ldg(T2 + e), s2);
+    }
+}
+
+// Phase 2: one warp per (task, B component, chunk of the (A component, aux
+// component) elements).  The lanes of a unit share b, so they share the term
+// list of the horizontal recurrence (built once per unit in shared memory) and
+// run its loops in lockstep.  The tile goes to its final place (integrals) or is
+// contracted with the adjoint (derivative; per-block partial gradients in shared
+// memory).
 template <bool DERIV>
 __global__ void __launch_bounds__(DFB_WARPS_PER_BLOCK * 32)
     k_rys_epi(ClassInfo ci, dfb_pair_side_t ps, dfb_aux_side_t ax, const int* __restrict__ task_pair,
@@ -319,21 +348,30 @@ __global__ void __launch_bounds__(DFB_WARPS_PER_BLOCK * 32)
               long sP, long sM, long sN, const double* __restrict__ bar, long sbP, long sbM, long sbN,
               double* __restrict__ grad, int natm, int smem_grad, const double* __restrict__ scratch, long slot) {
     extern __shared__ double sgrad[];
+    constexpr int NL = DERIV ? 4 : 1;  // term lists per warp: b, and b - 1_d for d = x, y, z
     const int lane = threadIdx.x & 31;
     const int wib = threadIdx.x >> 5;
     const int ngrad = (DERIV && smem_grad) ? natm * 3 : 0;
+    double* tc = sgrad + ngrad + wib * NL * DFB_HRR_TERMS;
+    int* tk = (int*)(sgrad + ngrad + DFB_WARPS_PER_BLOCK * NL * DFB_HRR_TERMS) + wib * NL * DFB_HRR_TERMS;
     const long gwarp = (long)blockIdx.x * DFB_WARPS_PER_BLOCK + wib;
     const long nwarps = (long)gridDim.x * DFB_WARPS_PER_BLOCK;
     if (DERIV && smem_grad) {
         for (int i = threadIdx.x; i < ngrad; i += blockDim.x) sgrad[i] = 0.0;
         __syncthreads();
     }
-    const int ntile = ci.na * ci.nb * ci.nc;
-    const int nec = (ntile + DFB_EPI_CHUNK - 1) / DFB_EPI_CHUNK;
+    const int ebase = -c_ncbtab[ci.lmin];
+    const int nf = ci.nf;
+    const int nac = ci.na * ci.nc;
+    const int nsub = (nac + DFB_EPI_CHUNK - 1) / DFB_EPI_CHUNK;
+    const int chunk = (((nac + nsub - 1) / nsub + 31) / 32) * 32;  // even chunks, whole passes of the warp
+    const int nec = ci.nb * nsub;
     for (long unit = gwarp; unit < nt * nec; unit += nwarps) {
         const long tl = unit / nec;
-        const int i0 = (int)(unit - tl * nec) * DFB_EPI_CHUNK;
-        const int i1 = (i0 + DFB_EPI_CHUNK < ntile) ? i0 + DFB_EPI_CHUNK : ntile;
+        const int r = (int)(unit - tl * nec);
+        const int ib = r / nsub;
+        const int j0 = (r - ib * nsub) * chunk;
+        const int j1 = (j0 + chunk < nac) ? j0 + chunk : nac;
         const long task = t0 + tl;
         long tp, ta;
         task_indices(task, naux_grid, tp, ta);
@@ -349,16 +387,26 @@ __global__ void __launch_bounds__(DFB_WARPS_PER_BLOCK * 32)
         const int aoB = ps.b_dummy ? 0 : ps.aostart[shB];
         const int aoC = ax.aostart[C];
         double gA[3] = {0.0, 0.0, 0.0}, gB[3] = {0.0, 0.0, 0.0};
-        for (int idx = i0 + lane; idx < i1; idx += 32) {
-            const int ic = idx % ci.nc;
-            const int iab = idx / ci.nc;
-            const int ib = iab % ci.nb;
-            const int ia = iab / ci.nb;
-            int a[3], b[3];
+        int b[3];
+        decode_cart(ci.lb, ib, b[0], b[1], b[2]);
+        __syncwarp();  // the previous unit's lanes are done with the lists
+        const int n0 = hrr_terms(b[0], b[1], b[2], AB, tc, tk, lane);
+        int nd[3] = {0, 0, 0};
+        if (DERIV) {
+            if (b[0] > 0) nd[0] = hrr_terms(b[0] - 1, b[1], b[2], AB, tc + DFB_HRR_TERMS, tk + DFB_HRR_TERMS, lane);
+            if (b[1] > 0)
+                nd[1] = hrr_terms(b[0], b[1] - 1, b[2], AB, tc + 2 * DFB_HRR_TERMS, tk + 2 * DFB_HRR_TERMS, lane);
+            if (b[2] > 0)
+                nd[2] = hrr_terms(b[0], b[1], b[2] - 1, AB, tc + 3 * DFB_HRR_TERMS, tk + 3 * DFB_HRR_TERMS, lane);
+        }
+        __syncwarp();
+        for (int j = j0 + lane; j < j1; j += 32) {
+            const int ia = j / ci.nc;
+            const int ic = j - ia * ci.nc;
+            int a[3];
             decode_cart(ci.la, ia, a[0], a[1], a[2]);
-            decode_cart(ci.lb, ib, b[0], b[1], b[2]);
             if (!DERIV) {
-                const double v = hrr(ci, E, a[0], a[1], a[2], b[0], b[1], b[2], ic, AB);
+                const double v = hrr_apply(E, nf, ic, ebase, a[0], a[1], a[2], tc, tk, n0);
                 if (mode == 0) {
                     const long P = aoC + ic, mu = aoA + ia, nu = aoB + ib;
                     out[P * sP + mu * sM + nu * sN] = v;
@@ -380,23 +428,27 @@ __global__ void __launch_bounds__(DFB_WARPS_PER_BLOCK * 32)
                     const double* WA = E + ci.nef;
                     const double* WB = E + 2 * ci.nef;
                     // (a b|c) of WB is shared by the three directions of the B derivative
-                    const double wb0 = ps.b_dummy ? 0.0 : hrr(ci, WB, a[0], a[1], a[2], b[0], b[1], b[2], ic, AB);
-                    // one direction per iteration, not unrolled: five HRR bodies in the
-                    // code instead of fifteen keeps the kernel inside the instruction cache
+                    const double wb0 = ps.b_dummy ? 0.0 : hrr_apply(WB, nf, ic, ebase, a[0], a[1], a[2], tc, tk, n0);
 #pragma unroll 1
                     for (int d = 0; d < 3; ++d) {
                         const int ex = d == 0, ey = d == 1, ez = d == 2;
                         const int ad = d == 0 ? a[0] : (d == 1 ? a[1] : a[2]);
                         const int bd = d == 0 ? b[0] : (d == 1 ? b[1] : b[2]);
                         const double abd = d == 0 ? AB[0] : (d == 1 ? AB[1] : AB[2]);
-                        double dA = hrr(ci, WA, a[0] + ex, a[1] + ey, a[2] + ez, b[0], b[1], b[2], ic, AB);
+                        double dA, dB;
+                        // d/dA: 2a (a+1_d b|c) - a_d (a-1_d b|c); d/dB: 2b (a+1_d b|c) + AB_d 2b (a b|c) - b_d (a b-1_d|c)
+                        hrr_apply2(WA, WB, nf, ic, ebase, a[0] + ex, a[1] + ey, a[2] + ez, tc, tk, n0, dA, dB);
                         if (ad > 0)
-                            dA -= (double)ad * hrr(ci, U, a[0] - ex, a[1] - ey, a[2] - ez, b[0], b[1], b[2], ic, AB);
-                        double dB = 0.0;
-                        if (!ps.b_dummy) {
-                            dB = hrr(ci, WB, a[0] + ex, a[1] + ey, a[2] + ez, b[0], b[1], b[2], ic, AB) + abd * wb0;
-                            if (bd > 0)
-                                dB -= (double)bd * hrr(ci, U, a[0], a[1], a[2], b[0] - ex, b[1] - ey, b[2] - ez, ic, AB);
+                            dA -= (double)ad * hrr_apply(U, nf, ic, ebase, a[0] - ex, a[1] - ey, a[2] - ez, tc, tk, n0);
+                        if (ps.b_dummy) {
+                            dB = 0.0;
+                        } else {
+                            dB += abd * wb0;
+                            if (bd > 0) {
+                                const int o = (d + 1) * DFB_HRR_TERMS;
+                                const int n = d == 0 ? nd[0] : (d == 1 ? nd[1] : nd[2]);
+                                dB -= (double)bd * hrr_apply(U, nf, ic, ebase, a[0], a[1], a[2], tc + o, tk + o, n);
+                            }
                         }
                         if (d == 0) {
                             gA[0] += gam * dA;
@@ -530,7 +582,8 @@ static int launch_rys(const ClassInfo& ci, const dfb_pair_side_t* ps, const dfb_
                          ci.lc, slot, scratch_doubles);
     const int smem_grad = (DERIV && natm * 3 <= 4096) ? 1 : 0;
     const size_t smem_acc = sizeof(double) * ((size_t)DFB_WARPS_PER_BLOCK * (32 * ci.item + ci.nr * 3 * ci.gt));
-    const size_t smem_epi = smem_grad ? sizeof(double) * natm * 3 : 0;
+    const size_t smem_epi = (smem_grad ? sizeof(double) * natm * 3 : 0) +
+                            (sizeof(double) + sizeof(int)) * DFB_WARPS_PER_BLOCK * (DERIV ? 4 : 1) * DFB_HRR_TERMS;
     auto kacc = k_rys_acc<KB, DERIV>;
     auto kepi = k_rys_epi<DERIV>;
     if (smem_acc > 48 * 1024) {
@@ -554,7 +607,7 @@ static int launch_rys(const ClassInfo& ci, const dfb_pair_side_t* ps, const dfb_
         kacc<<<(unsigned)b1, DFB_WARPS_PER_BLOCK * 32, smem_acc, st>>>(ci, *ps, *ax, task_pair, task_aux, t0, nt,
                                                                           naux_grid, scratch, slot,
                                                                           g_tables[dev].tab);
-        const long nec = (ci.na * ci.nb * ci.nc + DFB_EPI_CHUNK - 1) / DFB_EPI_CHUNK;
+        const long nec = (long)ci.nb * ((ci.na * ci.nc + DFB_EPI_CHUNK - 1) / DFB_EPI_CHUNK);
         long b2 = (nt * nec + DFB_WARPS_PER_BLOCK - 1) / DFB_WARPS_PER_BLOCK;
         if (b2 > (long)occ_epi * nsm) b2 = (long)occ_epi * nsm;
         kepi<<<(unsigned)b2, DFB_WARPS_PER_BLOCK * 32, smem_epi, st>>>(ci, *ps, *ax, task_pair, task_aux, t0, nt,
