@@ -38,6 +38,7 @@ import torch
 
 from . import basis as bm
 from . import geometry as geo
+from . import linalg as _la
 from . import mixed as _mixed
 from .df import DFEngine, ScratchHolder, cholesky_metric
 
@@ -53,6 +54,7 @@ class _Member:
     J: torch.Tensor      # static outputs (nao, nao)
     K: torch.Tensor
     Linv_split: tuple | None = None
+    Linv_blocks: list | None = None  # inverted diagonal blocks of L (block substitution)
 
 
 def water_cluster_batch(nmol: int = 64, nmin: int = 1, nmax: int = 16, basis: str = "ma-qzvp"):
@@ -100,6 +102,7 @@ class BatchedDFJK:
                         torch.zeros((nao, nocc), dtype=torch.float64, device=self.device),
                         torch.zeros((nao, nao), dtype=torch.float64, device=self.device),
                         torch.zeros((nao, nao), dtype=torch.float64, device=self.device))
+            m.Linv_blocks = _la.diag_block_inverses(L)
             if self.mixed_solve:
                 Linv = torch.linalg.solve_triangular(L, torch.eye(naux, dtype=L.dtype, device=L.device), upper=False)
                 m.Linv_split = _mixed.split3(Linv)
@@ -134,10 +137,7 @@ class BatchedDFJK:
                 c1 = min(nao * nocc, c0 + ncol)
                 Y[:, c0:c1] = _mixed.matmul(None, Y[:, c0:c1].contiguous(), kblock=4096, a_split=m.Linv_split)
         else:
-            ncol = max(nocc, ((1 << 28) // max(naux, 1)) // nocc * nocc)
-            for c0 in range(0, nao * nocc, ncol):
-                c1 = min(nao * nocc, c0 + ncol)
-                Y[:, c0:c1] = torch.linalg.solve_triangular(L, Y[:, c0:c1].contiguous(), upper=False)
+            _la.solve_lower(L, Y, m.Linv_blocks, out=Y)
         W3 = Y.view(naux, nao, nocc)
         K = m.K
         K.zero_()

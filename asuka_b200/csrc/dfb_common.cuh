@@ -49,15 +49,16 @@ __device__ __forceinline__ void task_indices(long t, long grid, long& tp, long& 
     }
 }
 
-// Nodes x_i (in t^2) and weights w_i (sum w_i = F_0(T)) of the n-point Rys rule.
-__device__ __forceinline__ void rys_eval(const RysTable& tab, int n, double T, double* x, double* w) {
+// Nodes x_i (in t^2) and weights w_i (sum w_i = F_0(T)) of the n-point Rys rule,
+// written to x[i * xs] and w[i * xs].
+__device__ __forceinline__ void rys_eval(const RysTable& tab, int n, double T, double* x, double* w, int xs = 1) {
     if (T >= tab.tmax) {
         const double* h = tab.herm + tab.hoff[n];
         const double inv = 1.0 / T;
         const double rs = rsqrt(T);
         for (int i = 0; i < n; ++i) {
-            x[i] = __ldg(h + i) * inv;
-            w[i] = __ldg(h + n + i) * rs;
+            x[i * xs] = __ldg(h + i) * inv;
+            w[i * xs] = __ldg(h + n + i) * rs;
         }
         return;
     }
@@ -72,9 +73,9 @@ __device__ __forceinline__ void rys_eval(const RysTable& tab, int n, double T, d
         double acc = __ldg(cr + tab.deg);
         for (int d = tab.deg - 1; d >= 0; --d) acc = fma(acc, u, __ldg(cr + d));
         if (r < n)
-            x[r] = acc;
+            x[r * xs] = acc;
         else
-            w[r - n] = acc;
+            w[(r - n) * xs] = acc;
     }
 }
 

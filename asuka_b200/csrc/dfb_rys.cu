@@ -209,37 +209,37 @@ __global__ void __launch_bounds__(DFB_WARPS_PER_BLOCK * 32, DFB_ACC_MIN_BLOCKS)
                 const double q = ax.pexp[c0 + ic];
                 const double inv = 1.0 / (p + q);
                 double PQ2 = 0.0;
-                double* it = items + lane * ci.item;
+                double* it = items + lane;  // field f of this lane's record at it[32 f]
                 it[0] = p;
-                it[1] = q;
+                it[32] = q;
 #pragma unroll
                 for (int d = 0; d < 3; ++d) {
                     const double cp = Cc[d] - Pp[d];
                     PQ2 += cp * cp;
-                    it[2 + d] = Pp[d] - A[d];
-                    it[5 + d] = cp;
+                    it[32 * (2 + d)] = Pp[d] - A[d];
+                    it[32 * (5 + d)] = cp;
                 }
                 const double T = p * q * inv * PQ2;
                 const double pref = kTwoPi52 / (p * q * sqrt(p + q)) * ps.cK[p0 + iab] * ax.pcoef[c0 + ic];
                 // nodes and weights straight into the lane's shared-memory record
-                rys_eval(tab, ci.nr, T, it + 8, it + 8 + ci.nr);
-                for (int u = 0; u < ci.nr; ++u) it[8 + ci.nr + u] *= pref;
+                rys_eval(tab, ci.nr, T, it + 32 * 8, it + 32 * (8 + ci.nr), 32);
+                for (int u = 0; u < ci.nr; ++u) it[32 * (8 + ci.nr + u)] *= pref;
             }
             __syncwarp();
             const int nb = (int)((nitems - base) < 32 ? (nitems - base) : 32);
             for (int jj = 0; jj < nb; ++jj) {
-                const double* it = items + jj * ci.item;
+                const double* it = items + jj;
                 if (lane < ci.nr * 3) {
                     const int u = lane / 3, d = lane - 3 * (lane / 3);
-                    const double p = it[0], q = it[1];
+                    const double p = it[0], q = it[32];
                     const double inv = 1.0 / (p + q);
-                    const double x = it[8 + u];
+                    const double x = it[32 * (8 + u)];
                     const double B0 = x * 0.5 * inv;
                     const double B1 = (1.0 - x) * 0.5 / p + B0;
                     const double B1p = (1.0 - x) * 0.5 / q + B0;
-                    const double Cd = it[2 + d] + (q * inv) * x * it[5 + d];
-                    const double Cpd = -(p * inv) * x * it[5 + d];
-                    const double g00 = (d == 0) ? it[8 + ci.nr + u] : 1.0;
+                    const double Cd = it[32 * (2 + d)] + (q * inv) * x * it[32 * (5 + d)];
+                    const double Cpd = -(p * inv) * x * it[32 * (5 + d)];
+                    const double g00 = (d == 0) ? it[32 * (8 + ci.nr + u)] : 1.0;
                     build_G(gtab + (u * 3 + d) * ci.gt, ci.nmax, ci.mmax, g00, Cd, Cpd, B0, B1, B1p);
                 }
                 __syncwarp();

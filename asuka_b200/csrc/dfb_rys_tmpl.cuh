@@ -116,8 +116,9 @@ __device__ __forceinline__ void rys_eval_t(const RysTable& tab, double T, double
 
 // Same evaluation, two table functions at a time, results to a per-thread
 // shared-memory slot r[0..NR) = nodes, r[NR..2NR) = weights (bounds the
-// coefficient registers in flight).
-template <int NR>
+// coefficient registers in flight); entry i sits at r[i * RS], so the slots of
+// consecutive threads interleave and a warp's stores hit consecutive words.
+template <int NR, int RS>
 __device__ __forceinline__ void rys_eval_smem(const RysTable& tab, double T, double* __restrict__ r) {
     if (T >= tab.tmax) {
         const double* h = tab.herm + tab.hoff[NR];
@@ -125,8 +126,8 @@ __device__ __forceinline__ void rys_eval_smem(const RysTable& tab, double T, dou
         const double rs = rsqrt(T);
 #pragma unroll
         for (int i = 0; i < NR; ++i) {
-            r[i] = __ldg(h + i) * inv;
-            r[NR + i] = __ldg(h + NR + i) * rs;
+            r[i * RS] = __ldg(h + i) * inv;
+            r[(NR + i) * RS] = __ldg(h + NR + i) * rs;
         }
         return;
     }
@@ -154,8 +155,8 @@ __device__ __forceinline__ void rys_eval_smem(const RysTable& tab, double T, dou
             a0 = fma(a0, u, cf0[d]);
             a1 = fma(a1, u, cf1[d]);
         }
-        r[f] = a0;
-        r[f + 1] = a1;
+        r[f * RS] = a0;
+        r[(f + 1) * RS] = a1;
     }
 }
 
@@ -418,7 +419,8 @@ __device__ __forceinline__ void rys_thread_body(const TmplArgs& g, long task, do
     constexpr int NR = CL::NR, NM = CL::NM, LB = CL::LB;
     // per-thread root slot after the optional gradient buffer
     extern __shared__ double smem_all[];
-    double* sroot = smem_all + ((CL::DERIV && g.smem_grad) ? g.natm * 3 : 0) + threadIdx.x * (2 * NR);
+    constexpr int RS = 128;  // threads per block: root slot entry i of thread t at sroot[i * 128]
+    double* sroot = smem_all + ((CL::DERIV && g.smem_grad) ? g.natm * 3 : 0) + threadIdx.x;
     long tp, ta;
     task_indices(task, g.naux_grid, tp, ta);
     const int pair = g.task_pair[tp];
@@ -467,7 +469,7 @@ __device__ __forceinline__ void rys_thread_body(const TmplArgs& g, long task, do
             if constexpr (NR <= 2)
                 rys_eval_t<NR>(g.tab, T, xr, wr);
             else
-                rys_eval_smem<NR>(g.tab, T, sroot);
+                rys_eval_smem<NR, RS>(g.tab, T, sroot);
             const double qi = q * inv, pi = p * inv;
             const double h_p = 0.5 / p, h_q = 0.5 / q;
 #pragma unroll
@@ -477,8 +479,8 @@ __device__ __forceinline__ void rys_thread_body(const TmplArgs& g, long task, do
                     x = xr[u < NRR ? u : 0];
                     wu = wr[u < NRR ? u : 0];
                 } else {
-                    x = sroot[u];
-                    wu = sroot[NR + u];
+                    x = sroot[u * RS];
+                    wu = sroot[(NR + u) * RS];
                 }
                 const double B0 = x * 0.5 * inv;
                 const double B1 = (1.0 - x) * h_p + B0;

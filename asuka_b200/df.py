@@ -31,6 +31,7 @@ import numpy as np
 import torch
 
 from . import _lib
+from . import linalg as _la
 from .basis import BasisCartSoA, build_shell_pairs_l_order, from_reference_like, ncart
 
 _DATA = os.path.join(os.path.dirname(os.path.abspath(__file__)), "data")
@@ -570,13 +571,12 @@ def whiten_3c2e(X: torch.Tensor, L: torch.Tensor, layout: str = "mnQ") -> torch.
     if layout == "mnQ":
         nao = X.shape[0]
         X2 = X.view(nao * nao, -1)
-        # B^T = L^-1 X^T  <=>  B = X L^-T
-        X2.copy_(torch.linalg.solve_triangular(L, X2.T, upper=False).T)
+        _la.solve_lower_right_T(L, X2, out=X2)  # B = X L^-T over the last index
         return X
     if layout == "Qmn":
         naux = X.shape[0]
         X2 = X.view(naux, -1)
-        X2.copy_(torch.linalg.solve_triangular(L, X2, upper=False))
+        _la.solve_lower(L, X2, out=X2)  # B_Q rows = L^-1 X
         return X
     raise ValueError("layout must be 'mnQ' or 'Qmn'")
 

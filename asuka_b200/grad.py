@@ -29,6 +29,7 @@ from __future__ import annotations
 import numpy as np
 import torch
 
+from . import linalg as _la
 from . import mixed as _mixed
 from .df import DFEngine, cholesky_metric
 
@@ -37,48 +38,63 @@ def _mm(A, B, precision):
     return A @ B if precision == "fp64" else _mixed.matmul(A, B)
 
 
-def df_forward(engine: DFEngine, Cw: torch.Tensor, precision: str = "fp64", X: torch.Tensor | None = None):
-    """Integrals at the engine's current geometry, then (E_2e, J, K) and the saved intermediates.
+def _nomark(_key: str) -> None:
+    pass
 
-    With D = Cw Cw^T the Coulomb density rho_P = <X_P, D> = sum Cw * (X_P Cw) is read
-    from Y = X Cw (needed for K anyway) instead of a second pass over X.
-    """
-    nao, naux = engine.nao, engine.naux
-    nocc = Cw.shape[1]
+
+def df_forward(engine: DFEngine, Cw: torch.Tensor, precision: str = "fp64", X: torch.Tensor | None = None):
+    """Integrals at the engine's current geometry, then (E_2e, J, K) and the saved intermediates."""
     V = engine.metric()
     L = cholesky_metric(V)
     X = engine.int3c("Qmn", out=X)
+    return df_contract(engine, Cw, X, L, precision)
+
+
+def df_contract(engine: DFEngine, Cw: torch.Tensor, X: torch.Tensor, L: torch.Tensor, precision: str = "fp64",
+                mark=_nomark):
+    """(E_2e, J, K) and the saved intermediates from the 3c tensor X ('Qmn') and the metric factor L.
+
+    With D = Cw Cw^T the Coulomb density rho_P = <X_P, D> = sum Cw * (X_P Cw) is read
+    from Y = X Cw (needed for K anyway) instead of a second pass over X.  ``mark(name)``
+    is called after each phase (timing hooks).
+    """
+    nao, naux = engine.nao, engine.naux
+    nocc = Cw.shape[1]
     X2 = X.view(naux, nao * nao)
     D = Cw @ Cw.T
     D = 0.5 * (D + D.T)
     Y = (X.view(naux * nao, nao) @ Cw).view(naux, nao * nocc)
+    mark("jk_Y")
     rho = Y @ Cw.reshape(-1)
     d = torch.cholesky_solve(rho.view(-1, 1), L).view(-1)
     J = (d @ X2).view(nao, nao)
     J = 0.5 * (J + J.T)
+    mark("jk_rho_J")
+    Linv_blocks = _la.diag_block_inverses(L)
     if precision == "fp64":
-        W = torch.linalg.solve_triangular(L, Y, upper=False)
+        W = _la.solve_lower(L, Y, Linv_blocks, out=Y)
     else:
         # mixed: the compute-bound solve as a split-BF16 GEMM with L^-1
         Linv = torch.linalg.solve_triangular(L, torch.eye(naux, dtype=L.dtype, device=L.device), upper=False)
         W = _mixed.matmul(Linv, Y, kblock=4096)
+    mark("jk_W_solve")
     W2 = W.view(naux, nao, nocc).permute(1, 0, 2).reshape(nao, naux * nocc)
     K = _mixed.syrk(W2) if precision != "fp64" else W2 @ W2.T
     K = 0.5 * (K + K.T)
     E = 0.5 * torch.dot(rho, d) - 0.25 * torch.sum(D * K)
-    return E, J, K, dict(X=X, L=L, d=d, W=W, D=D)
+    mark("jk_K")
+    return E, J, K, dict(X=X, L=L, d=d, W=W, D=D, Linv_blocks=Linv_blocks)
 
 
-def df_backward(engine: DFEngine, Cw: torch.Tensor, saved: dict, grad: torch.Tensor | None = None,
-                precision: str = "fp64") -> torch.Tensor:
-    """dE_2e/dR accumulated into grad (natm, 3)."""
+def df_adjoints(engine: DFEngine, Cw: torch.Tensor, saved: dict):
+    """Adjoints of the 3c and 2c integrals: (Gamma (naux, nao, nao), written over X; G2 (naux, naux))."""
     nao, naux = engine.nao, engine.naux
     nocc = Cw.shape[1]
-    X, L, d, W, D = saved["X"], saved["L"], saved["d"], saved["W"], saved["D"]
+    X, L, d, W = saved["X"], saved["L"], saved["d"], saved["W"]
     # M_Q = Cw^T W_Q  (naux, nocc, nocc)
     M = torch.matmul(Cw.T, W.view(naux, nao, nocc))
     M = 0.5 * (M + M.transpose(1, 2))
-    Z = torch.linalg.solve_triangular(L.T, M.reshape(naux, nocc * nocc), upper=True)
+    Z = _la.solve_lower_T(L, M.reshape(naux, nocc * nocc), saved.get("Linv_blocks"))
     Zq = Z.view(naux, nocc, nocc)
     # Gamma_P = d_P D - 1/2 Cw Z_P Cw^T = Cw (d_P I - 1/2 Z_P) Cw^T since D = Cw Cw^T:
     # one batched GEMM, written over X's storage (X is not needed afterwards)
@@ -87,8 +103,15 @@ def df_backward(engine: DFEngine, Cw: torch.Tensor, saved: dict, grad: torch.Ten
     G3 = X
     torch.matmul(Cw, T, out=G3)
     G2 = -0.5 * torch.outer(d, d) + 0.25 * (Z @ Z.T)
+    return G3, G2
+
+
+def df_backward(engine: DFEngine, Cw: torch.Tensor, saved: dict, grad: torch.Tensor | None = None,
+                precision: str = "fp64") -> torch.Tensor:
+    """dE_2e/dR accumulated into grad (natm, 3)."""
+    G3, G2 = df_adjoints(engine, Cw, saved)
     if grad is None:
-        grad = torch.zeros((engine.natm, 3), dtype=torch.float64, device=X.device)
+        grad = torch.zeros((engine.natm, 3), dtype=torch.float64, device=G3.device)
     engine.deriv3c(G3, grad, layout="Qmn")
     engine.deriv2c(G2, grad)
     return grad
@@ -125,18 +148,16 @@ def df_energy(coords: torch.Tensor, Cw: torch.Tensor, engine: DFEngine, precisio
 # ---------------------------------------------------------------- streamed (B never stored)
 
 def _solve_lower_inplace(L: torch.Tensor, Y: torch.Tensor, precision: str, ncol: int = 1 << 18) -> torch.Tensor:
-    """Y <- L^-1 Y in place, by column blocks (one block copy alive at a time).
+    """Y <- L^-1 Y in place.
 
-    FP64: triangular solves.  Mixed: L^-1 formed once in FP64, split once into
-    BF16 terms, and applied to each column block as a split-BF16 GEMM.
+    FP64: block substitution (``asuka_b200.linalg``).  Mixed: L^-1 formed once in
+    FP64, split once into BF16 terms, and applied to each column block as a
+    split-BF16 GEMM (one block copy alive at a time).
     """
     n, m = Y.shape
     ncol = max(1, min(m, ncol * 1024 // max(n, 1)))
     if precision == "fp64":
-        for c0 in range(0, m, ncol):
-            c1 = min(m, c0 + ncol)
-            Y[:, c0:c1] = torch.linalg.solve_triangular(L, Y[:, c0:c1].contiguous(), upper=False)
-        return Y
+        return _la.solve_lower(L, Y, out=Y)
     Linv = torch.linalg.solve_triangular(L, torch.eye(n, dtype=L.dtype, device=L.device), upper=False)
     sp = _mixed.split3(Linv)
     del Linv
@@ -199,7 +220,7 @@ def df_energy_grad_streamed(engine: DFEngine, Cw: torch.Tensor, aux_block: int =
     for q0 in range(0, naux, qb):
         Mc = M[q0:q0 + qb]
         Mc.copy_(0.5 * (Mc + Mc.transpose(1, 2)))
-    Z = torch.linalg.solve_triangular(L.T, M.view(naux, nocc * nocc), upper=True)
+    Z = _la.solve_lower_T(L, M.view(naux, nocc * nocc))
     del M
     Zq = Z.view(naux, nocc, nocc)
     grad = torch.zeros((engine.natm, 3), dtype=torch.float64, device=dev)

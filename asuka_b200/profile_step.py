@@ -18,7 +18,7 @@ import torch
 from . import basis as bm
 from . import geometry as geo
 from .df import DFEngine, cholesky_metric
-from .grad import df_backward, df_forward
+from .grad import df_adjoints, df_contract
 
 WORKLOADS = {
     "w8": lambda: geo.water_cluster(8, 0, "ma-tzvp"),
@@ -61,10 +61,8 @@ def phases(eng: DFEngine, Cw: torch.Tensor, R: torch.Tensor, precision: str, X: 
     mark("cholesky")
     eng.int3c("Qmn", out=X)
     mark("int3c")
-    # contractions (same algebra as grad.df_forward/df_backward)
-    E, J, K, saved = df_forward_from_X(eng, Cw, precision, X, L, mark)
-    mark("jk_K")
-    G3, G2 = adjoints(eng, Cw, saved)
+    E, J, K, saved = df_contract(eng, Cw, X, L, precision, mark)
+    G3, G2 = df_adjoints(eng, Cw, saved)
     mark("adjoints")
     grad = torch.zeros((eng.natm, 3), dtype=torch.float64, device="cuda")
     eng.deriv3c(G3, grad)
@@ -76,46 +74,6 @@ def phases(eng: DFEngine, Cw: torch.Tensor, R: torch.Tensor, precision: str, X: 
     out = {k: ev[keys[i - 1]].elapsed_time(ev[k]) for i, k in enumerate(keys) if i > 0}
     out["total"] = ev["start"].elapsed_time(ev[keys[-1]])
     return out
-
-
-def df_forward_from_X(eng, Cw, precision, X, L, mark=lambda k: None):
-    from . import mixed as _mixed
-
-    nao, naux = eng.nao, eng.naux
-    nocc = Cw.shape[1]
-    X2 = X.view(naux, nao * nao)
-    D = Cw @ Cw.T
-    mm = (lambda A, B: A @ B) if precision == "fp64" else _mixed.matmul
-    Y = (X.view(naux * nao, nao) @ Cw).view(naux, nao * nocc)
-    mark("jk_Y")
-    rho = Y @ Cw.reshape(-1)
-    d = torch.cholesky_solve(rho.view(-1, 1), L).view(-1)
-    J = (d @ X2).view(nao, nao)
-    mark("jk_rho_J")
-    if precision == "fp64":
-        W = torch.linalg.solve_triangular(L, Y, upper=False)
-    else:
-        Linv = torch.linalg.solve_triangular(L, torch.eye(naux, dtype=L.dtype, device=L.device), upper=False)
-        W = _mixed.matmul(Linv, Y, kblock=4096)
-    mark("jk_W_trsm")
-    W2 = W.view(naux, nao, nocc).permute(1, 0, 2).reshape(nao, naux * nocc)
-    K = mm(W2, W2.T) if precision == "fp64" else _mixed.syrk(W2)
-    E = 0.5 * torch.dot(rho, d) - 0.25 * torch.sum(D * K)
-    return E, J, K, dict(X=X, L=L, d=d, W=W, D=D)
-
-
-def adjoints(eng, Cw, saved):
-    nao, naux = eng.nao, eng.naux
-    nocc = Cw.shape[1]
-    X, L, d, W, D = saved["X"], saved["L"], saved["d"], saved["W"], saved["D"]
-    M = torch.matmul(Cw.T, W.view(naux, nao, nocc))
-    M = 0.5 * (M + M.transpose(1, 2))
-    Z = torch.linalg.solve_triangular(L.T, M.reshape(naux, nocc * nocc), upper=True)
-    Zp = -0.5 * Z.view(naux, nocc, nocc) + d.view(naux, 1, 1) * torch.eye(nocc, dtype=Z.dtype, device=Z.device)
-    T = torch.matmul(Zp, Cw.T)
-    torch.matmul(Cw, T, out=X)
-    G2 = -0.5 * torch.outer(d, d) + 0.25 * (Z @ Z.T)
-    return X, G2
 
 
 def class_times(eng, mol, top: int = 20) -> dict:

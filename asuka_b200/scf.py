@@ -25,6 +25,7 @@ from typing import Any
 import numpy as np
 import torch
 
+from . import linalg as _la
 from . import basis as bm
 from .df import DFEngine, cholesky_metric, whiten_3c2e
 from .geometry import Molecule
@@ -250,7 +251,7 @@ def _direct_jk(engine: DFEngine, L: torch.Tensor, aux_block: int = 256):
             y[p0:p1] = Xb.view(p1 - p0, -1) @ D.reshape(-1)
             YT[p0:p1] = torch.matmul(Xb.view(-1, nao), Cw).view(p1 - p0, -1)
         w = torch.cholesky_solve(y.view(-1, 1), L).view(-1)
-        W = torch.linalg.solve_triangular(L, YT, upper=False)
+        W = _la.solve_lower(L, YT, out=YT)
         W2 = W.view(naux, nao, nocc).permute(1, 0, 2).reshape(nao, -1)
         K = _sym(W2 @ W2.T)
         J = torch.zeros((nao, nao), dtype=torch.float64, device=D.device)

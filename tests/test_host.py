@@ -73,3 +73,31 @@ def test_engine_methods_called_are_defined():
     assigned = set(re.findall(r"self\.(\w+)\s*=", src))
     missing = sorted(n for n in called if not hasattr(df.DFEngine, n) and n not in assigned)
     assert not missing, missing
+
+
+def test_block_substitution_matches_triangular_solve():
+    """The blocked solves (used on the device) agree with a plain triangular solve."""
+    import torch
+
+    from asuka_b200 import linalg
+
+    g = torch.Generator().manual_seed(0)
+    n = 700  # three blocks of 256, the last one ragged
+    A = torch.randn(n, n, generator=g, dtype=torch.float64)
+    L = torch.linalg.cholesky(A @ A.T + n * torch.eye(n, dtype=torch.float64))
+    Y = torch.randn(n, 37, generator=g, dtype=torch.float64)
+    ref = torch.linalg.solve_triangular(L, Y, upper=False)
+    inv = linalg.diag_block_inverses(L)
+    assert torch.allclose(linalg.solve_lower(L, Y, inv), ref, rtol=0, atol=1e-12 * float(ref.abs().max()))
+    Yc = Y.clone()
+    linalg.solve_lower(L, Yc, inv, out=Yc)  # in place
+    assert torch.allclose(Yc, ref, rtol=0, atol=1e-12 * float(ref.abs().max()))
+    refT = torch.linalg.solve_triangular(L.T, Y, upper=True)
+    Mc = Y.clone()
+    linalg.solve_lower_T(L, Mc, inv, out=Mc)
+    assert torch.allclose(Mc, refT, rtol=0, atol=1e-12 * float(refT.abs().max()))
+    X = torch.randn(29, n, generator=g, dtype=torch.float64)
+    refR = torch.linalg.solve_triangular(L, X.T, upper=False).T
+    Xc = X.clone()
+    linalg.solve_lower_right_T(L, Xc, inv, out=Xc)
+    assert torch.allclose(Xc, refR, rtol=0, atol=1e-12 * float(refR.abs().max()))
