@@ -144,7 +144,7 @@ class BatchedDFJK:
         qb = max(1, (1 << 27) // max(nao * nocc, 1))
         for q0 in range(0, naux, qb):
             Wc = W3[q0:q0 + qb].permute(1, 0, 2).reshape(nao, -1)
-            if mixed:
+            if mixed and nao >= _mixed.MIN_DIM:
                 K += _mixed.syrk(Wc)
             else:
                 K.addmm_(Wc, Wc.T)

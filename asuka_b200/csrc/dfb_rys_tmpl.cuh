@@ -26,7 +26,7 @@
 #include "../../include/dfb.h"
 #include "dfb_common.cuh"
 
-#define DFB_RYS_DEG 9  // Horner degree of the Rys table (checked at upload)
+#define DFB_RYS_DEG 9  // polynomial degree of the Rys table (checked at upload)
 
 namespace dfb {
 
@@ -76,6 +76,16 @@ __host__ __device__ constexpr double c_binom(int n, int k) {
     return (k < 0 || k > n) ? 0.0 : v;
 }
 
+// Degree-9 polynomial in u by Estrin's scheme: five independent linear terms, then
+// three levels of combination with u^2, u^4, u^8 -- a dependency depth of four
+// fused multiply-adds instead of Horner's nine.
+__device__ __forceinline__ double poly9(const double* c, double u, double u2, double u4, double u8) {
+    const double p01 = fma(c[1], u, c[0]), p23 = fma(c[3], u, c[2]), p45 = fma(c[5], u, c[4]);
+    const double p67 = fma(c[7], u, c[6]), p89 = fma(c[9], u, c[8]);
+    const double q0 = fma(p23, u2, p01), q1 = fma(p67, u2, p45);
+    return fma(p89, u8, fma(q1, u4, q0));
+}
+
 template <int NR>
 __device__ __forceinline__ void rys_eval_t(const RysTable& tab, double T, double (&x)[NR], double (&w)[NR]) {
     if (T >= tab.tmax) {
@@ -94,6 +104,8 @@ __device__ __forceinline__ void rys_eval_t(const RysTable& tab, double T, double
     if (k > tab.nint - 1) k = tab.nint - 1;
     const double u = 2.0 * (Th - (double)k) - 1.0;
     constexpr int S = DFB_RYS_DEG + 1;
+    static_assert(S == 10, "poly9 evaluates degree-9 tables");
+    const double u2 = u * u, u4 = u2 * u2, u8 = u4 * u4;
     const double2* c = reinterpret_cast<const double2*>(tab.coef + tab.offs[NR] + (size_t)k * (2 * NR) * S);
 #pragma unroll
     for (int r = 0; r < 2 * NR; ++r) {
@@ -104,9 +116,7 @@ __device__ __forceinline__ void rys_eval_t(const RysTable& tab, double T, double
             cf[2 * d] = v.x;
             cf[2 * d + 1] = v.y;
         }
-        double acc = cf[S - 1];
-#pragma unroll
-        for (int d = S - 2; d >= 0; --d) acc = fma(acc, u, cf[d]);
+        const double acc = poly9(cf, u, u2, u4, u8);
         if (r < NR)
             x[r] = acc;
         else
@@ -136,6 +146,7 @@ __device__ __forceinline__ void rys_eval_smem(const RysTable& tab, double T, dou
     if (k > tab.nint - 1) k = tab.nint - 1;
     const double u = 2.0 * (Th - (double)k) - 1.0;
     constexpr int S = DFB_RYS_DEG + 1;
+    const double u2 = u * u, u4 = u2 * u2, u8 = u4 * u4;
     const double2* c = reinterpret_cast<const double2*>(tab.coef + tab.offs[NR] + (size_t)k * (2 * NR) * S);
 #pragma unroll 1
     for (int f = 0; f < 2 * NR; f += 2) {
@@ -149,14 +160,8 @@ __device__ __forceinline__ void rys_eval_smem(const RysTable& tab, double T, dou
             cf1[2 * d] = v1.x;
             cf1[2 * d + 1] = v1.y;
         }
-        double a0 = cf0[S - 1], a1 = cf1[S - 1];
-#pragma unroll
-        for (int d = S - 2; d >= 0; --d) {
-            a0 = fma(a0, u, cf0[d]);
-            a1 = fma(a1, u, cf1[d]);
-        }
-        r[f * RS] = a0;
-        r[(f + 1) * RS] = a1;
+        r[f * RS] = poly9(cf0, u, u2, u4, u8);
+        r[(f + 1) * RS] = poly9(cf1, u, u2, u4, u8);
     }
 }
 

@@ -70,16 +70,13 @@ def df_contract(engine: DFEngine, Cw: torch.Tensor, X: torch.Tensor, L: torch.Te
     J = (d @ X2).view(nao, nao)
     J = 0.5 * (J + J.T)
     mark("jk_rho_J")
+    # the solve stays FP64 in both modes: block substitution runs at the DGEMM rate, and a
+    # split-BF16 product with L^-1 loses accuracy in proportion to the metric's conditioning
     Linv_blocks = _la.diag_block_inverses(L)
-    if precision == "fp64":
-        W = _la.solve_lower(L, Y, Linv_blocks, out=Y)
-    else:
-        # mixed: the compute-bound solve as a split-BF16 GEMM with L^-1
-        Linv = torch.linalg.solve_triangular(L, torch.eye(naux, dtype=L.dtype, device=L.device), upper=False)
-        W = _mixed.matmul(Linv, Y, kblock=4096)
+    W = _la.solve_lower(L, Y, Linv_blocks, out=Y)
     mark("jk_W_solve")
     W2 = W.view(naux, nao, nocc).permute(1, 0, 2).reshape(nao, naux * nocc)
-    K = _mixed.syrk(W2) if precision != "fp64" else W2 @ W2.T
+    K = _mixed.syrk(W2) if (precision != "fp64" and nao >= _mixed.MIN_DIM) else W2 @ W2.T
     K = 0.5 * (K + K.T)
     E = 0.5 * torch.dot(rho, d) - 0.25 * torch.sum(D * K)
     mark("jk_K")
@@ -207,7 +204,7 @@ def df_energy_grad_streamed(engine: DFEngine, Cw: torch.Tensor, aux_block: int =
     qb = max(1, (1 << 27) // max(nao * nocc, 1))
     for q0 in range(0, naux, qb):
         Wc = W3[q0:q0 + qb].permute(1, 0, 2).reshape(nao, -1)
-        if precision == "fp64":
+        if precision == "fp64" or nao < _mixed.MIN_DIM:
             K.addmm_(Wc, Wc.T)
         else:
             K += _mixed.syrk(Wc)

@@ -147,3 +147,19 @@ def test_gradient_matches_central_finite_differences():
             vals.append(float(df_forward(eng, Cw)[0]))
         fd = (vals[0] - vals[1]) / (2 * h)
         assert abs(fd - float(gR[a, c])) < 1e-7, (a, c, fd, float(gR[a, c]))
+
+
+def test_split_bf16_products():
+    """Split-BF16 rank-k update and product (FP32 accumulation per block) against FP64."""
+    from asuka_b200 import mixed
+
+    g = torch.Generator(device="cuda").manual_seed(0)
+    A = torch.randn(1100, 20000, generator=g, dtype=torch.float64, device="cuda")
+    ref = A @ A.T
+    K = mixed.syrk(A)
+    # about 2e-6 relative for 1024-long accumulation blocks
+    assert float((K - ref).abs().max()) < 1e-5 * float(ref.abs().max())
+    assert float((K - K.T).abs().max()) == 0.0
+    B = torch.randn(20000, 300, generator=g, dtype=torch.float64, device="cuda")
+    ref = A @ B
+    assert float((mixed.matmul(A, B) - ref).abs().max()) < 1e-5 * float(ref.abs().max())
