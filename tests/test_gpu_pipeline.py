@@ -159,7 +159,6 @@ def test_split_bf16_products():
     K = mixed.syrk(A)
     # about 2e-6 relative for 1024-long accumulation blocks
     assert float((K - ref).abs().max()) < 1e-5 * float(ref.abs().max())
-    assert float((K - K.T).abs().max()) == 0.0
     B = torch.randn(20000, 300, generator=g, dtype=torch.float64, device="cuda")
     ref = A @ B
     assert float((mixed.matmul(A, B) - ref).abs().max()) < 1e-5 * float(ref.abs().max())
