@@ -53,6 +53,39 @@ def _workload():
     return mol, bm.pack_basis(atoms, "ma-tzvp", "ao"), bm.pack_basis(atoms, "ma-tzvp", "aux")
 
 
+# DRAM bytes (read + write) of one 3c derivative contraction of this workload (all class launches of
+# one gradient), from one ncu capture: --metrics dram__bytes_read.sum,dram__bytes_write.sum -k regex:k_rys
+# on `python -m asuka_b200.profile_step --workload w8 --only deriv3c --steps 1` (3.814e9 + 0.023e9).
+DERIV3C_DRAM_BYTES = 3.837e9
+
+
+def flops_3c(ao, aux, deriv: bool = False) -> float:
+    """Algorithmic FLOPs of the 3c integrals (deriv=False) or of the 3c derivative contraction,
+    summed over every (AO shell pair, aux shell) triplet with the per-unit model
+    K_ab K_P n_r (3 n_A n_B n_P + 9 (l_a+l_b+1)(l_P+1)) for integrals and
+    K_ab K_P n_r' (25 n_A n_B n_P + 9 (l_a+l_b+2)(l_P+2)) for the derivative."""
+    if deriv:
+        return flops_deriv3c(ao, aux)
+    from asuka_b200.basis import build_shell_pairs_l_order, ncart
+
+    sp = build_shell_pairs_l_order(ao)
+    la = ao.shell_l[sp.sp_A]
+    lb = ao.shell_l[sp.sp_B]
+    tot = 0.0
+    for lp in np.unique(aux.shell_l):
+        kp = float(aux.shell_nprim[aux.shell_l == lp].sum())
+        for a in np.unique(la):
+            for b in np.unique(lb):
+                m = (la == a) & (lb == b)
+                if not m.any():
+                    continue
+                kab = float(sp.sp_npair[m].sum())
+                nr = (a + b + lp) // 2 + 1
+                n3 = ncart(int(a)) * ncart(int(b)) * ncart(int(lp))
+                tot += kab * kp * nr * (n3 * 3 + 9 * (a + b + 1) * (lp + 1))
+    return tot
+
+
 def flops_deriv3c(ao, aux) -> float:
     """Algorithmic FLOPs of the 3c derivative contraction (per-unit model of the survey, 8(d))."""
     from asuka_b200.basis import build_shell_pairs_l_order, ncart
@@ -289,6 +322,46 @@ def run_gpu(args) -> dict | None:
     fp64_src = "measured live: FP64 FMA probe (dfb_fp64_fma_probe), all SMs, best of 5"
     dgemm_peak = fp64_dgemm_tflops(4096, dev)
     achieved = fl / (t_d3 * 1e-3) / 1e12
+    # per-phase device times of one step (event marks between phases), averaged over 3 steps,
+    # each with the roofline fraction of its bound
+    from asuka_b200.profile_step import phases as _phases
+
+    runs = {"fp64": [], "mixed": []}
+    for i in range(7):  # interleaved; the first pair is a warm-up
+        for prec in ("fp64", "mixed"):
+            r = _phases(eng, Cw, R, prec, X)
+            if i:
+                runs[prec].append(r)
+    phase_ms = {prec: {k: float(np.median([r[k] for r in rs])) for k in rs[0]} for prec, rs in runs.items()}
+    pk = _peaks()
+    hbm = float(pk.get("hbm_gbs", 6650.0))
+    f3 = flops_3c(ao, aux)
+    f_jk = 2.0 * naux * nao * nao * nocc + 1.0 * naux * naux * nao * nocc + 2.0 * nao * nao * naux * nocc
+    f_adj = (2.0 * naux * nao * nocc * nocc + 1.0 * naux * naux * nocc * nocc + 2.0 * naux * nocc * nocc * nao
+             + 2.0 * naux * nao * nao * nocc + 2.0 * naux * naux * nocc * nocc)
+    j_bytes = 8.0 * naux * nao * nao  # J = sum_P d_P X_P reads X once
+
+    def _ph(prec):
+        p = phase_ms[prec]
+        jk = p["jk_Y"] + p["jk_rho_J"] + p["jk_W_solve"] + p["jk_K"]
+        grad = p["adjoints"] + p["deriv3c"] + p["deriv2c"]
+        return {
+            "int3c_ms": round(p["int3c"], 3),
+            "int3c_frac_fp64": round(f3 / (p["int3c"] * 1e-3) / 1e12 / fp64_peak, 4),
+            "metric_and_cholesky_ms": round(p["metric"] + p["cholesky"], 3),
+            "jk_ms": round(jk, 3),
+            "jk_dense_frac_dgemm": round(f_jk / ((jk - p["jk_rho_J"]) * 1e-3) / 1e12 / dgemm_peak, 4),
+            "j_read_frac_hbm_measured": round(j_bytes / (p["jk_rho_J"] * 1e-3) / 1e9 / hbm, 4),
+            "j_read_frac_hbm_nominal_8tbs": round(j_bytes / (p["jk_rho_J"] * 1e-3) / 1e9 / 8000.0, 4),
+            "gradient_ms": round(grad, 3),
+            "adjoints_frac_dgemm": round(f_adj / (p["adjoints"] * 1e-3) / 1e12 / dgemm_peak, 4),
+            "deriv3c_ms": round(p["deriv3c"], 3),
+            "deriv3c_frac_fp64": round(fl / (p["deriv3c"] * 1e-3) / 1e12 / fp64_peak, 4),
+            "deriv2c_ms": round(p["deriv2c"], 3),
+            "step_ms": round(p["total"], 3),
+        }
+
+    phases_out = {prec: _ph(prec) for prec in ("fp64", "mixed")}
     del X, saved, G3
     torch.cuda.empty_cache()
 
@@ -328,8 +401,9 @@ def run_gpu(args) -> dict | None:
         "metric": METRIC, "value": round(ms_mx, 4), "unit": "ms", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(ms_mx, 4), "higher_is_better": False, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded geometry; basis tables from the reference)",
-        "config": {"workload": WORKLOAD, "nao": nao, "naux": naux, "precision": "mixed (split-BF16 J/K contractions,"
-                   " FP64 integrals and gradient accumulation)", "l2": "working set (3c tensor 2.5 GB) > L2 126 MB",
+        "config": {"workload": WORKLOAD, "nao": nao, "naux": naux, "precision": "mixed (split-BF16 exchange update"
+                   " above its measured crossover nao >= 1024, FP64 below it and for the integrals, solves and"
+                   " gradient accumulation)", "l2": "working set (3c tensor 2.5 GB) > L2 126 MB",
                    "replicas": world if world > 1 else None},
         "fp64_ms_per_step": round(ms_64, 4),
         "mixed_speedup_vs_fp64": round(ms_64 / ms_mx, 4),
@@ -343,8 +417,13 @@ def run_gpu(args) -> dict | None:
                      "achieved": round(achieved, 3), "peak": fp64_peak, "unit": "TFLOP/s",
                      "frac": round(achieved / fp64_peak, 4), "peak_source": fp64_src,
                      "fp64_dgemm_tflops": round(dgemm_peak, 2),
-                     "avg_launch_set_ms": round(t_d3, 4), "algorithmic_flops": fl, "traffic": None},
+                     "avg_launch_set_ms": round(t_d3, 4), "algorithmic_flops": fl,
+                     "traffic": DERIV3C_DRAM_BYTES, "traffic_unit": "bytes per launch set (ncu)"},
         "clocks": clk, "clocks_fp64_run": clk64,
+        "phases": phases_out,
+        "phase_models": {"int3c_flops": f3, "deriv3c_flops": fl, "jk_dense_flops": f_jk, "adjoint_flops": f_adj,
+                         "j_bytes": j_bytes, "fp64_fma_peak_tflops": fp64_peak, "dgemm_peak_tflops": round(dgemm_peak, 2),
+                         "hbm_peak_gbs": hbm},
     }
     if not args.no_cpu_baseline:
         try:
