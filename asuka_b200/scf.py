@@ -237,28 +237,15 @@ def pack_B_to_Qp(B: torch.Tensor, layout: str = "Qmn") -> torch.Tensor:
 
 
 def _direct_jk(engine: DFEngine, L: torch.Tensor, aux_block: int = 256):
-    """Streamed DF J/K (``asuka/hf/df_jk_streamed.py:167-325``): the 3c integrals are recomputed
-    per aux block in two passes per cycle and B is never stored."""
-    nao, naux = engine.nao, engine.naux
-    blocks = engine.aux_blocks(aux_block)
+    """Streamed DF J/K for the SCF (``asuka/hf/df_jk_streamed.py:167-325``): the 3c integrals are
+    recomputed per aux block in two passes per cycle and B is never stored."""
+    from .streamed import df_JK_streamed, make_streamed_df_jk_context
+
+    ctx = make_streamed_df_jk_context(engine.ao, engine.aux, aux_block_naux=aux_block, engine=engine, L_metric=L)
 
     def jk(D, Cw, prec):
-        nocc = Cw.shape[1]
-        y = torch.empty(naux, dtype=torch.float64, device=D.device)
-        YT = torch.empty((naux, nao * nocc), dtype=torch.float64, device=D.device)
-        for (p0, p1, shells) in blocks:
-            Xb = engine.int3c_block(shells, p0, p1)  # (p1-p0, nao, nao)
-            y[p0:p1] = Xb.view(p1 - p0, -1) @ D.reshape(-1)
-            YT[p0:p1] = torch.matmul(Xb.view(-1, nao), Cw).view(p1 - p0, -1)
-        w = torch.cholesky_solve(y.view(-1, 1), L).view(-1)
-        W = _la.solve_lower(L, YT, out=YT)
-        W2 = W.view(naux, nao, nocc).permute(1, 0, 2).reshape(nao, -1)
-        K = _sym(W2 @ W2.T)
-        J = torch.zeros((nao, nao), dtype=torch.float64, device=D.device)
-        for (p0, p1, shells) in blocks:
-            Xb = engine.int3c_block(shells, p0, p1)
-            J += (w[p0:p1] @ Xb.view(p1 - p0, -1)).view(nao, nao)
-        return _sym(J), K
+        ones = torch.ones(Cw.shape[1], dtype=torch.float64, device=Cw.device)
+        return df_JK_streamed(ctx, D, Cw, ones, precision=prec)
 
     return jk
 

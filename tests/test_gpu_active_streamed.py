@@ -1,0 +1,67 @@
+"""Active-space DF factors (CASSCF consumer) and streamed J/K with several occupied sets (UHF)."""
+
+import numpy as np
+import pytest
+
+from _util import bases_of, golden
+
+pytestmark = pytest.mark.gpu
+torch = pytest.importorskip("torch")
+
+
+def _stored(g):
+    from asuka_b200.df import DFEngine, cholesky_metric, whiten_3c2e
+
+    ao, aux, sp = bases_of(g)
+    eng = DFEngine(ao, aux)
+    L = cholesky_metric(eng.metric())
+    BQ = whiten_3c2e(eng.int3c("Qmn"), L, layout="Qmn")
+    return ao, aux, eng, L, BQ
+
+
+@pytest.mark.parametrize("name", ["h2o_masvp", "n2_masvp"])
+def test_active_factors_all_layouts(name):
+    from asuka_b200.active import (active_Lfull_from_B, active_Lfull_from_B_Qp, active_Lfull_from_cached_B_whitened,
+                                   active_Lfull_streamed_basis)
+    from asuka_b200.scf import pack_B_to_Qp
+
+    g = golden(name)
+    ao, aux, eng, L, BQ = _stored(g)
+    C = torch.as_tensor(g["mo_coeff"], device="cuda")[:, 2:8].contiguous()  # a 6-orbital active space
+    norb, naux = C.shape[1], BQ.shape[0]
+    # plain reference: L[p q, Q] = sum_mn C_mp C_nq B_Q[m, n]
+    ref = np.einsum("mp,nq,Qmn->pqQ", C.cpu().numpy(), C.cpu().numpy(), BQ.cpu().numpy()).reshape(norb * norb, naux)
+    scale = np.abs(ref).max()
+    B_mnQ = BQ.permute(1, 2, 0).contiguous()
+    for Lf in (active_Lfull_from_B(B_mnQ, C), active_Lfull_from_B(BQ, C, layout="Qmn"),
+               active_Lfull_from_cached_B_whitened(B_mnQ, C),
+               active_Lfull_from_B_Qp(pack_B_to_Qp(BQ), C, aux_block_naux=7),
+               active_Lfull_from_cached_B_whitened(pack_B_to_Qp(BQ), C)):
+        assert Lf.shape == (norb * norb, naux)
+        assert np.abs(Lf.cpu().numpy() - ref).max() < 1e-12 * scale
+    Ls = active_Lfull_streamed_basis(ao, aux, C, aux_block_naux=40)
+    assert np.abs(Ls.cpu().numpy() - ref).max() < 1e-11 * scale
+
+
+@pytest.mark.parametrize("aux_block", [32, 100000])
+def test_streamed_jks_two_occupied_sets(aux_block):
+    from asuka_b200.jk import df_J_from_BQ_D, df_K_from_BQ_Cw
+    from asuka_b200.streamed import df_JK_streamed, df_JKs_streamed, make_streamed_df_jk_context
+
+    g = golden("h2o_matzvp")
+    ao, aux, eng, L, BQ = _stored(g)
+    C = torch.as_tensor(g["mo_coeff"], device="cuda")
+    nocc = int((g["mo_occ"] > 0).sum())
+    Ca, Cb = C[:, :nocc], C[:, :nocc - 1]  # a doublet-like pair of occupied sets
+    occa = torch.ones(nocc, dtype=torch.float64, device="cuda")
+    occb = torch.ones(nocc - 1, dtype=torch.float64, device="cuda")
+    D = Ca @ Ca.T + Cb @ Cb.T
+    ctx = make_streamed_df_jk_context(ao, aux, aux_block_naux=aux_block, engine=eng, L_metric=L)
+    J, (Ka, Kb) = df_JKs_streamed(ctx, D, [Ca, Cb], [occa, occb], k_q_block=17)
+    J0 = df_J_from_BQ_D(BQ, D)
+    scale = float(J0.abs().max())
+    assert float((J - J0).abs().max()) < 1e-11 * scale
+    assert float((Ka - df_K_from_BQ_Cw(BQ, Ca.contiguous())).abs().max()) < 1e-11 * scale
+    assert float((Kb - df_K_from_BQ_Cw(BQ, Cb.contiguous())).abs().max()) < 1e-11 * scale
+    J1, K1 = df_JK_streamed(ctx, D, Ca, occa)
+    assert float((J1 - J).abs().max()) < 1e-12 * scale and float((K1 - Ka).abs().max()) < 1e-12 * scale
