@@ -538,15 +538,32 @@ def metric_2c2e_basis(aux_basis, *, stream=None, backend: str = "gpu_rys", mode:
     return eng.metric()
 
 
+def _check_ao_rep(ao_rep: str) -> str:
+    if ao_rep not in ("cart", "sph"):
+        raise ValueError("ao_rep must be 'cart' or 'sph'")
+    return ao_rep
+
+
 def int3c2e_basis(ao_basis, aux_basis, *, stream=None, backend: str = "gpu_rys", mode: str = "warp",
-                  threads: int = 256, mixed_precision: bool = False, layout: str = "mnQ") -> torch.Tensor:
-    """X[mu,nu,P] = (mu nu|P) (``asuka/cueri/df.py:859``); layout 'mnQ' or 'Qmn'."""
+                  threads: int = 256, mixed_precision: bool = False, layout: str = "mnQ",
+                  ao_rep: str = "cart") -> torch.Tensor:
+    """X[mu,nu,P] = (mu nu|P) (``asuka/cueri/df.py:859``); layout 'mnQ' or 'Qmn'.
+
+    ``ao_rep='sph'`` returns X over real spherical AOs (the aux index stays Cartesian).
+    """
+    _check_ao_rep(ao_rep)
     ao, aux = _as_soa(ao_basis), _as_soa(aux_basis)
     if ao.shell_atom is None:
         ao = from_reference_like(ao, np.zeros(ao.nshell, np.int32))
     if aux.shell_atom is None:
         aux = from_reference_like(aux, np.zeros(aux.nshell, np.int32))
-    return DFEngine(ao, aux).int3c(layout)
+    eng = DFEngine(ao, aux)
+    if ao_rep == "cart":
+        return eng.int3c(layout)
+    from .sph import cart2sph_ao_matrix, int3c_cart_to_sph
+
+    return int3c_cart_to_sph(eng.int3c("Qmn"), cart2sph_ao_matrix(ao.shell_l, eng.device),
+                             "Qmn").permute(*((1, 2, 0) if layout == "mnQ" else (0, 1, 2))).contiguous()
 
 
 def cholesky_metric(V: torch.Tensor, *, shift: float = 0.0) -> torch.Tensor:
@@ -588,8 +605,7 @@ def build_df_B_from_cueri_packed_bases(ao_basis, aux_basis, *, config=None, layo
     FP64 device tensors; ``layout='mnQ'`` -> (nao, nao, naux), ``'Qmn'`` -> (naux, nao, nao).
     Errors raise RuntimeError/ValueError/NotImplementedError; there is no CPU fallback.
     """
-    if ao_rep != "cart":
-        raise NotImplementedError("ao_rep='sph' is not implemented (Cartesian AOs only)")
+    _check_ao_rep(ao_rep)
     ao, aux = _as_soa(ao_basis), _as_soa(aux_basis)
     if ao.shell_atom is None:
         ao = from_reference_like(ao, np.zeros(ao.nshell, np.int32))
@@ -602,7 +618,14 @@ def build_df_B_from_cueri_packed_bases(ao_basis, aux_basis, *, config=None, layo
     V = eng.metric()
     if ev:
         ev[1].record()
-    X = eng.int3c(layout)
+    if ao_rep == "cart":
+        X = eng.int3c(layout)
+    else:  # real spherical AOs on the AO side; the aux index stays Cartesian
+        from .sph import cart2sph_ao_matrix, int3c_cart_to_sph
+
+        X = int3c_cart_to_sph(eng.int3c("Qmn"), cart2sph_ao_matrix(ao.shell_l, eng.device), "Qmn")
+        if layout == "mnQ":
+            X = X.permute(1, 2, 0).contiguous()
     if ev:
         ev[2].record()
     L = cholesky_metric(V)

@@ -17,7 +17,10 @@ Every fixture is produced by the reference's own public CPU path:
   density, with ``bar_L[Q] = rho_Q D - 1/2 D B_Q D``;
 * ``_eri_rys_cpu.eri_rys_tile_cart_sp_batch_cy`` for single (ab|P) and (P|Q)
   tiles of every angular class of H2O/ma-QZVP;
-* ``_eri_rys_cpu.rys_roots_weights_cy`` for reference roots/weights.
+* ``_eri_rys_cpu.rys_roots_weights_cy`` for reference roots/weights;
+* ``asuka.cueri.sph.cart2sph_matrix`` (``asuka/cueri/sph.py:95``) for the
+  Cartesian-to-spherical transforms of l = 0..5 (pure Python; importable
+  straight from the source tree).
 
 Geometries come from ``asuka_b200.geometry`` so that tests rebuild identical
 inputs without the reference.
@@ -164,12 +167,20 @@ def roots_case() -> None:
     print("ref_roots: done", flush=True)
 
 
+def sph_case() -> None:
+    from asuka.cueri.sph import cart2sph_matrix
+
+    np.savez_compressed(os.path.join(HERE, "cart2sph_ref.npz"),
+                        **{f"l{l}": np.asarray(cart2sph_matrix(l)) for l in range(6)})
+
+
 CASES = {
     "n2_masvp": lambda: scf_case("n2_masvp", geo.n2("ma-svp")),
     "h2o_masvp": lambda: scf_case("h2o_masvp", geo.water("ma-svp")),
     "h2o_matzvp": lambda: scf_case("h2o_matzvp", geo.water("ma-tzvp")),
     "tiles_h2o_maqzvp": lambda: tiles_case("tiles_h2o_maqzvp", geo.water("ma-qzvp")),
     "ref_roots": roots_case,
+    "cart2sph_ref": sph_case,
 }
 
 if __name__ == "__main__":

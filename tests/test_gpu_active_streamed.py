@@ -65,3 +65,27 @@ def test_streamed_jks_two_occupied_sets(aux_block):
     assert float((Kb - df_K_from_BQ_Cw(BQ, Cb.contiguous())).abs().max()) < 1e-11 * scale
     J1, K1 = df_JK_streamed(ctx, D, Ca, occa)
     assert float((J1 - J).abs().max()) < 1e-12 * scale and float((K1 - Ka).abs().max()) < 1e-12 * scale
+
+
+@pytest.mark.parametrize("layout", ["mnQ", "Qmn"])
+def test_spherical_ao_factors(layout):
+    """ao_rep='sph': X over real spherical AOs = T^T X_cart T against the reference X (oracle-pinned)."""
+    from _util import unpack_tril
+    from asuka_b200.df import build_df_B_from_cueri_packed_bases, cholesky_metric, int3c2e_basis
+    from asuka_b200.sph import cart2sph_ao_matrix, sph_coeff_sph_to_cart
+
+    g = golden("h2o_matzvp")  # d and f AO shells
+    ao, aux, sp = bases_of(g)
+    Xs = int3c2e_basis(ao, aux, layout=layout, ao_rep="sph")
+    T = cart2sph_ao_matrix(ao.shell_l).numpy()
+    nao = T.shape[0]
+    Xc = unpack_tril(g["X_tril"], nao)  # (nao, nao, naux) from the reference
+    ref = np.einsum("ms,nt,mnP->stP", T, T, Xc)
+    got = Xs.cpu().numpy() if layout == "mnQ" else Xs.permute(1, 2, 0).cpu().numpy()
+    assert got.shape == ref.shape
+    assert np.abs(got - ref).max() < 1e-11 * np.abs(ref).max()
+    B, L = build_df_B_from_cueri_packed_bases(ao, aux, layout="mnQ", ao_rep="sph", return_L=True)
+    Bref = np.linalg.solve(L.cpu().numpy(), ref.reshape(-1, ref.shape[2]).T).T.reshape(ref.shape)
+    assert np.abs(B.cpu().numpy() - Bref).max() < 1e-10 * np.abs(Bref).max()
+    Cs = torch.randn(T.shape[1], 4, dtype=torch.float64, device="cuda")
+    assert np.abs(sph_coeff_sph_to_cart(Cs, ao.shell_l).cpu().numpy() - T @ Cs.cpu().numpy()).max() < 1e-13
