@@ -174,7 +174,9 @@ def main():
         return
     phases(eng, Cw, R, args.precision, X)  # warm-up
     res = [phases(eng, Cw, R, args.precision, X) for _ in range(args.steps)]
-    avg = {k: float(np.mean([r[k] for r in res])) for k in res[0]}
+    # median over steps: a step whose host side fell behind the device (page faults, the
+    # allocator, Python) would otherwise inflate the phase it happened in
+    avg = {k: float(np.median([r[k] for r in res])) for k in res[0]}
     print(json.dumps({"workload": args.workload, "nao": eng.nao, "naux": eng.naux, "precision": args.precision,
                       "ms": {k: round(v, 3) for k, v in avg.items()}}))
 
