@@ -10,7 +10,8 @@ import ctypes
 import os
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(_HERE, "libdfb.so")
+# DFB_LIB_PATH selects another build of the same library (the class tuner's variant build)
+LIB_PATH = os.environ.get("DFB_LIB_PATH") or os.path.join(_HERE, "libdfb.so")
 
 _d = ctypes.c_void_p  # device pointers travel as integers
 

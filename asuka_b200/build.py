@@ -75,5 +75,35 @@ def build(force: bool = False, verbose: bool = False, jobs: int | None = None) -
     return OUT
 
 
+def build_variant(defines: list[str], out: str, tag: str, jobs: int | None = None) -> str:
+    """A second library whose class-specialised kernels are compiled with extra -D defines
+    (objects in _build_<tag>); the other sources reuse the main build's objects."""
+    build()
+    nvcc = os.environ.get("NVCC", "nvcc")
+    objdir = os.path.join(HERE, "_build")
+    vdir = os.path.join(HERE, f"_build_{tag}")
+    os.makedirs(vdir, exist_ok=True)
+    compile_flags = [f for f in NVCC_FLAGS if f not in ("--shared", "-lcublas")] + [f"-D{d}" for d in defines]
+    objs, procs = [], []
+    jobs = jobs or max(1, os.cpu_count() or 1)
+    for src in sources():
+        base = os.path.basename(src)[:-3]
+        if not base.startswith("dfb_cls_"):
+            objs.append(os.path.join(objdir, base + ".o"))
+            continue
+        obj = os.path.join(vdir, base + ".o")
+        objs.append(obj)
+        while len([p for p in procs if p.poll() is None]) >= jobs:
+            procs[0].wait() if procs[0].poll() is None else procs.pop(0)
+        procs.append(subprocess.Popen([nvcc, *compile_flags, "-c", src, "-o", obj], cwd=CSRC))
+    for p in procs:
+        if p.wait() != 0:
+            raise RuntimeError(f"nvcc failed: {p.args}")
+    os.makedirs(os.path.dirname(out), exist_ok=True)
+    subprocess.run([nvcc, "-gencode", "arch=compute_100a,code=sm_100a", "--shared", "-o", out, *objs],
+                   check=True, cwd=CSRC)
+    return out
+
+
 if __name__ == "__main__":
     print(build(force="--force" in sys.argv, verbose=True))

@@ -5,31 +5,31 @@ namespace dfb {
 int dfb_cls_d0_launch(int la, int lb, int lc, const TmplArgs& g, long nblk, size_t smem, cudaStream_t st) {
     (void)la;
     if (lb == 0 && lc == 0) {
-        k_rys_thread<0, 0, 0, 1, true, false><<<dim3((unsigned)nblk, 1), 128, smem, st>>>(g);
+        k_rys_thread<0, 0, 0, 1, true, false, 1><<<dim3((unsigned)nblk, 1), 128, smem, st>>>(g);
         return 1;
     }
     if (lb == 0 && lc == 1) {
-        k_rys_thread<0, 0, 1, 1, true, false><<<dim3((unsigned)nblk, 1), 128, smem, st>>>(g);
+        k_rys_thread<0, 0, 1, 1, true, false, 1><<<dim3((unsigned)nblk, 1), 128, smem, st>>>(g);
         return 1;
     }
     if (lb == 0 && lc == 2) {
-        k_rys_thread<0, 0, 2, 2, true, false><<<dim3((unsigned)nblk, 2), 128, smem, st>>>(g);
+        k_rys_thread<0, 0, 2, 2, true, false, 1><<<dim3((unsigned)nblk, 2), 128, smem, st>>>(g);
         return 1;
     }
     if (lb == 0 && lc == 3) {
-        k_rys_thread<0, 0, 3, 2, true, false><<<dim3((unsigned)nblk, 2), 128, smem, st>>>(g);
+        k_rys_thread<0, 0, 3, 2, true, false, 1><<<dim3((unsigned)nblk, 2), 128, smem, st>>>(g);
         return 1;
     }
     if (lb == 0 && lc == 4) {
-        k_rys_thread<0, 0, 4, 3, true, false><<<dim3((unsigned)nblk, 3), 128, smem, st>>>(g);
+        k_rys_thread<0, 0, 4, 3, true, false, 1><<<dim3((unsigned)nblk, 3), 128, smem, st>>>(g);
         return 1;
     }
     if (lb == 0 && lc == 5) {
-        k_rys_thread<0, 0, 5, 5, true, false><<<dim3((unsigned)nblk, 5), 128, smem, st>>>(g);
+        k_rys_thread<0, 0, 5, 5, true, false, 1><<<dim3((unsigned)nblk, 5), 128, smem, st>>>(g);
         return 1;
     }
     if (lb == 0 && lc == 6) {
-        k_rys_thread<0, 0, 6, 6, true, false><<<dim3((unsigned)nblk, 6), 128, smem, st>>>(g);
+        k_rys_thread<0, 0, 6, 6, true, false, 1><<<dim3((unsigned)nblk, 6), 128, smem, st>>>(g);
         return 1;
     }
     return 0;

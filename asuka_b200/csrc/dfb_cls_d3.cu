@@ -5,55 +5,55 @@ namespace dfb {
 int dfb_cls_d3_launch(int la, int lb, int lc, const TmplArgs& g, long nblk, size_t smem, cudaStream_t st) {
     (void)la;
     if (lb == 0 && lc == 0) {
-        k_rys_thread<3, 0, 0, 1, true, true><<<dim3((unsigned)nblk, 2), 128, smem, st>>>(g);
+        k_rys_thread<3, 0, 0, 1, true, true, 1><<<dim3((unsigned)nblk, 2), 128, smem, st>>>(g);
         return 1;
     }
     if (lb == 0 && lc == 1) {
-        k_rys_thread<3, 0, 1, 2, true, true><<<dim3((unsigned)nblk, 4), 128, smem, st>>>(g);
+        k_rys_thread<3, 0, 1, 2, true, true, 1><<<dim3((unsigned)nblk, 4), 128, smem, st>>>(g);
         return 1;
     }
     if (lb == 0 && lc == 2) {
-        k_rys_thread<3, 0, 2, 3, true, true><<<dim3((unsigned)nblk, 6), 128, smem, st>>>(g);
+        k_rys_thread<3, 0, 2, 3, true, true, 1><<<dim3((unsigned)nblk, 6), 128, smem, st>>>(g);
         return 1;
     }
     if (lb == 0 && lc == 3) {
-        k_rys_thread<3, 0, 3, 5, true, true><<<dim3((unsigned)nblk, 10), 128, smem, st>>>(g);
+        k_rys_thread<3, 0, 3, 5, true, true, 1><<<dim3((unsigned)nblk, 10), 128, smem, st>>>(g);
         return 1;
     }
     if (lb == 0 && lc == 4) {
-        k_rys_thread<3, 0, 4, 8, true, true><<<dim3((unsigned)nblk, 16), 128, smem, st>>>(g);
+        k_rys_thread<3, 0, 4, 8, true, true, 1><<<dim3((unsigned)nblk, 16), 128, smem, st>>>(g);
         return 1;
     }
     if (lb == 0 && lc == 5) {
-        k_rys_thread<3, 0, 5, 21, true, true><<<dim3((unsigned)nblk, 42), 128, smem, st>>>(g);
+        k_rys_thread<3, 0, 5, 21, true, true, 1><<<dim3((unsigned)nblk, 42), 128, smem, st>>>(g);
         return 1;
     }
     if (lb == 0 && lc == 6) {
-        k_rys_thread<3, 0, 6, 28, true, true><<<dim3((unsigned)nblk, 56), 128, smem, st>>>(g);
+        k_rys_thread<3, 0, 6, 28, true, true, 1><<<dim3((unsigned)nblk, 56), 128, smem, st>>>(g);
         return 1;
     }
     if (lb == 1 && lc == 0) {
-        k_rys_thread<3, 1, 0, 1, true, true><<<dim3((unsigned)nblk, 2), 128, smem, st>>>(g);
+        k_rys_thread<3, 1, 0, 1, true, true, 1><<<dim3((unsigned)nblk, 2), 128, smem, st>>>(g);
         return 1;
     }
     if (lb == 1 && lc == 1) {
-        k_rys_thread<3, 1, 1, 3, true, true><<<dim3((unsigned)nblk, 6), 128, smem, st>>>(g);
+        k_rys_thread<3, 1, 1, 3, true, true, 1><<<dim3((unsigned)nblk, 6), 128, smem, st>>>(g);
         return 1;
     }
     if (lb == 1 && lc == 2) {
-        k_rys_thread<3, 1, 2, 6, true, true><<<dim3((unsigned)nblk, 12), 128, smem, st>>>(g);
+        k_rys_thread<3, 1, 2, 6, true, true, 1><<<dim3((unsigned)nblk, 12), 128, smem, st>>>(g);
         return 1;
     }
     if (lb == 1 && lc == 3) {
-        k_rys_thread<3, 1, 3, 10, true, true><<<dim3((unsigned)nblk, 20), 128, smem, st>>>(g);
+        k_rys_thread<3, 1, 3, 10, true, true, 1><<<dim3((unsigned)nblk, 20), 128, smem, st>>>(g);
         return 1;
     }
     if (lb == 1 && lc == 4) {
-        k_rys_thread<3, 1, 4, 15, true, true><<<dim3((unsigned)nblk, 30), 128, smem, st>>>(g);
+        k_rys_thread<3, 1, 4, 15, true, true, 1><<<dim3((unsigned)nblk, 30), 128, smem, st>>>(g);
         return 1;
     }
     if (lb == 1 && lc == 5) {
-        k_rys_thread<3, 1, 5, 21, true, true><<<dim3((unsigned)nblk, 42), 128, smem, st>>>(g);
+        k_rys_thread<3, 1, 5, 21, true, true, 1><<<dim3((unsigned)nblk, 42), 128, smem, st>>>(g);
         return 1;
     }
     return 0;

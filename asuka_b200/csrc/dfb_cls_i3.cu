@@ -5,59 +5,59 @@ namespace dfb {
 int dfb_cls_i3_launch(int la, int lb, int lc, const TmplArgs& g, long nblk, size_t smem, cudaStream_t st) {
     (void)la;
     if (lb == 0 && lc == 0) {
-        k_rys_thread<3, 0, 0, 1, false, false><<<dim3((unsigned)nblk, 1), 128, smem, st>>>(g);
+        k_rys_thread<3, 0, 0, 1, false, false, 1><<<dim3((unsigned)nblk, 1), 128, smem, st>>>(g);
         return 1;
     }
     if (lb == 0 && lc == 1) {
-        k_rys_thread<3, 0, 1, 1, false, false><<<dim3((unsigned)nblk, 1), 128, smem, st>>>(g);
+        k_rys_thread<3, 0, 1, 1, false, false, 1><<<dim3((unsigned)nblk, 1), 128, smem, st>>>(g);
         return 1;
     }
     if (lb == 0 && lc == 2) {
-        k_rys_thread<3, 0, 2, 2, false, false><<<dim3((unsigned)nblk, 2), 128, smem, st>>>(g);
+        k_rys_thread<3, 0, 2, 2, false, false, 1><<<dim3((unsigned)nblk, 2), 128, smem, st>>>(g);
         return 1;
     }
     if (lb == 0 && lc == 3) {
-        k_rys_thread<3, 0, 3, 3, false, false><<<dim3((unsigned)nblk, 3), 128, smem, st>>>(g);
+        k_rys_thread<3, 0, 3, 3, false, false, 1><<<dim3((unsigned)nblk, 3), 128, smem, st>>>(g);
         return 1;
     }
     if (lb == 0 && lc == 4) {
-        k_rys_thread<3, 0, 4, 4, false, false><<<dim3((unsigned)nblk, 4), 128, smem, st>>>(g);
+        k_rys_thread<3, 0, 4, 4, false, false, 1><<<dim3((unsigned)nblk, 4), 128, smem, st>>>(g);
         return 1;
     }
     if (lb == 0 && lc == 5) {
-        k_rys_thread<3, 0, 5, 7, false, false><<<dim3((unsigned)nblk, 7), 128, smem, st>>>(g);
+        k_rys_thread<3, 0, 5, 7, false, false, 1><<<dim3((unsigned)nblk, 7), 128, smem, st>>>(g);
         return 1;
     }
     if (lb == 0 && lc == 6) {
-        k_rys_thread<3, 0, 6, 28, false, false><<<dim3((unsigned)nblk, 28), 128, smem, st>>>(g);
+        k_rys_thread<3, 0, 6, 28, false, false, 1><<<dim3((unsigned)nblk, 28), 128, smem, st>>>(g);
         return 1;
     }
     if (lb == 1 && lc == 0) {
-        k_rys_thread<3, 1, 0, 1, false, false><<<dim3((unsigned)nblk, 1), 128, smem, st>>>(g);
+        k_rys_thread<3, 1, 0, 1, false, false, 1><<<dim3((unsigned)nblk, 1), 128, smem, st>>>(g);
         return 1;
     }
     if (lb == 1 && lc == 1) {
-        k_rys_thread<3, 1, 1, 3, false, false><<<dim3((unsigned)nblk, 3), 128, smem, st>>>(g);
+        k_rys_thread<3, 1, 1, 3, false, false, 1><<<dim3((unsigned)nblk, 3), 128, smem, st>>>(g);
         return 1;
     }
     if (lb == 1 && lc == 2) {
-        k_rys_thread<3, 1, 2, 6, false, false><<<dim3((unsigned)nblk, 6), 128, smem, st>>>(g);
+        k_rys_thread<3, 1, 2, 6, false, false, 1><<<dim3((unsigned)nblk, 6), 128, smem, st>>>(g);
         return 1;
     }
     if (lb == 1 && lc == 3) {
-        k_rys_thread<3, 1, 3, 10, false, false><<<dim3((unsigned)nblk, 10), 128, smem, st>>>(g);
+        k_rys_thread<3, 1, 3, 10, false, false, 1><<<dim3((unsigned)nblk, 10), 128, smem, st>>>(g);
         return 1;
     }
     if (lb == 1 && lc == 4) {
-        k_rys_thread<3, 1, 4, 15, false, false><<<dim3((unsigned)nblk, 15), 128, smem, st>>>(g);
+        k_rys_thread<3, 1, 4, 15, false, false, 1><<<dim3((unsigned)nblk, 15), 128, smem, st>>>(g);
         return 1;
     }
     if (lb == 1 && lc == 5) {
-        k_rys_thread<3, 1, 5, 21, false, false><<<dim3((unsigned)nblk, 21), 128, smem, st>>>(g);
+        k_rys_thread<3, 1, 5, 21, false, false, 1><<<dim3((unsigned)nblk, 21), 128, smem, st>>>(g);
         return 1;
     }
     if (lb == 1 && lc == 6) {
-        k_rys_thread<3, 1, 6, 28, false, false><<<dim3((unsigned)nblk, 28), 128, smem, st>>>(g);
+        k_rys_thread<3, 1, 6, 28, false, false, 1><<<dim3((unsigned)nblk, 28), 128, smem, st>>>(g);
         return 1;
     }
     return 0;

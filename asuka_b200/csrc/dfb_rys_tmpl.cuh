@@ -546,11 +546,15 @@ __device__ __forceinline__ void rys_thread_body(const TmplArgs& g, long task, do
 
 // grid.y enumerates (pass, component subset): SPLIT derivative classes run the
 // centre-A pass on y < FS and the centre-B pass on FS <= y < 2 FS.
+// MINB: resident 128-thread blocks per SM the register allocation must allow, chosen per class
+// from measured timings (csrc/class_tuning.json, written by asuka_b200.tune_classes);
+// DFB_THREAD_MIN_BLOCKS raises it for every class (the tuner's variant build).
 #ifndef DFB_THREAD_MIN_BLOCKS
-#define DFB_THREAD_MIN_BLOCKS 1  // resident 128-thread blocks per SM the register allocation must allow
+#define DFB_THREAD_MIN_BLOCKS 1
 #endif
-template <int LA, int LB, int LC, int FS, bool DERIV, bool SPLIT>
-__global__ void __launch_bounds__(128, DFB_THREAD_MIN_BLOCKS) k_rys_thread(TmplArgs g) {
+template <int LA, int LB, int LC, int FS, bool DERIV, bool SPLIT, int MINB = 1>
+__global__ void __launch_bounds__(128, (DFB_THREAD_MIN_BLOCKS > MINB ? DFB_THREAD_MIN_BLOCKS : MINB))
+    k_rys_thread(TmplArgs g) {
     extern __shared__ double sgrad[];
     const int ng = (DERIV && g.smem_grad) ? g.natm * 3 : 0;
     if (DERIV && g.smem_grad) {

@@ -75,7 +75,19 @@ def plan(la, lb, lc, deriv):
     return None
 
 
+def tuning() -> dict:
+    """Per-class launch-bounds choices measured by asuka_b200.tune_classes (empty when absent)."""
+    import json
+
+    p = os.path.join(HERE, "class_tuning.json")
+    if not os.path.exists(p):
+        return {}
+    with open(p) as f:
+        return json.load(f).get("min_blocks", {})
+
+
 def main() -> None:
+    tune = tuning()
     for old in os.listdir(HERE):
         if old.startswith("dfb_cls_") and old.endswith(".cu"):
             os.remove(os.path.join(HERE, old))
@@ -101,7 +113,9 @@ def main() -> None:
                 "    (void)la;",
             ]
             for (a, b, c, fs, split) in cls:
-                kern = f"k_rys_thread<{a}, {b}, {c}, {fs}, {'true' if deriv else 'false'}, {'true' if split else 'false'}>"
+                minb = int(tune.get(f"{'d' if deriv else 'i'}{a}{b}{c}", 1))
+                kern = (f"k_rys_thread<{a}, {b}, {c}, {fs}, {'true' if deriv else 'false'}, "
+                        f"{'true' if split else 'false'}, {minb}>")
                 lines.append(f"    if (lb == {b} && lc == {c}) {{")
                 lines.append(f"        {kern}<<<dim3((unsigned)nblk, {fs * (2 if split else 1)}), 128, smem, st>>>(g);")
                 lines.append("        return 1;")

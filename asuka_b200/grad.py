@@ -245,6 +245,26 @@ def df_energy_grad_streamed(engine: DFEngine, Cw: torch.Tensor, aux_block: int =
 
 # ---------------------------------------------------------------- reference seam
 
+def whitened_adjoints(B: torch.Tensor, barL: torch.Tensor, L: torch.Tensor):
+    """Backprop dE/dB through the whitening and the metric Cholesky.
+
+    B (nao, nao, naux) whitened factors, barL (naux, nao, nao) = dE/dB, L the metric
+    factor -> (bar_X (naux, nao, nao) symmetric, bar_V (naux, naux) symmetric), the
+    adjoints of the unwhitened integrals X and of the metric V
+    (``asuka/integrals/df_adjoint.py:172-235,322-361``).
+    """
+    nao, _, naux = B.shape
+    tmp = _la.solve_lower_T(L, barL.reshape(naux, nao * nao))  # L^-T bar_B^T
+    bar_Lc = -torch.tril(tmp @ B.reshape(nao * nao, naux))
+    bar_X = tmp.view(naux, nao, nao)
+    bar_X = 0.5 * (bar_X + bar_X.transpose(1, 2))
+    G = torch.tril(L.T @ bar_Lc)
+    G.diagonal().mul_(0.5)
+    t2 = torch.linalg.solve_triangular(L.T, G, upper=True)
+    bar_V = torch.linalg.solve_triangular(L.T, t2.T, upper=True).T
+    return bar_X.contiguous(), (0.5 * (bar_V + bar_V.T)).contiguous()
+
+
 def compute_df_gradient_contributions_analytic_packed_bases(ao_basis, aux_basis, *, atom_coords_bohr, B_ao,
                                                             bar_L_ao, L_chol=None, backend: str = "cuda",
                                                             df_threads: int = 0, profile: dict | None = None):
@@ -270,16 +290,8 @@ def compute_df_gradient_contributions_analytic_packed_bases(ao_basis, aux_basis,
         L = torch.as_tensor(L_chol, dtype=torch.float64, device=dev)
     else:
         L = cholesky_metric(eng.metric())
-    tmp = torch.linalg.solve_triangular(L.T, barL.view(naux, nao * nao), upper=True)  # L^-T bar_B^T
-    bar_Lc = -torch.tril(tmp @ B.view(nao * nao, naux))
-    bar_X = tmp.view(naux, nao, nao)
-    bar_X = 0.5 * (bar_X + bar_X.transpose(1, 2))
-    G = torch.tril(L.T @ bar_Lc)
-    G.diagonal().mul_(0.5)
-    t2 = torch.linalg.solve_triangular(L.T, G, upper=True)
-    bar_V = torch.linalg.solve_triangular(L.T, t2.T, upper=True).T
-    bar_V = 0.5 * (bar_V + bar_V.T)
+    bar_X, bar_V = whitened_adjoints(B, barL, L)
     grad = torch.zeros((natm, 3), dtype=torch.float64, device=dev)
-    eng.deriv3c(bar_X.contiguous(), grad, layout="Qmn")
-    eng.deriv2c(bar_V.contiguous(), grad)
+    eng.deriv3c(bar_X, grad, layout="Qmn")
+    eng.deriv2c(bar_V, grad)
     return grad.cpu().numpy()

@@ -162,3 +162,36 @@ def test_split_bf16_products():
     B = torch.randn(20000, 300, generator=g, dtype=torch.float64, device="cuda")
     ref = A @ B
     assert float((mixed.matmul(A, B) - ref).abs().max()) < 1e-5 * float(ref.abs().max())
+
+
+def test_gradient_context_layouts():
+    """The reusable gradient context gives the reference gradient from mnQ, packed-Qp and
+    split-term inputs, and its spherical-AO contraction equals the Cartesian one."""
+    from asuka_b200.df import DFEngine, cholesky_metric, whiten_3c2e
+    from asuka_b200.grad_context import DFGradContractionContext
+    from asuka_b200.scf import pack_B_to_Qp
+    from asuka_b200.sph import cart2sph_ao_matrix
+
+    g = golden("h2o_masvp")
+    ao, aux, sp = bases_of(g)
+    eng = DFEngine(ao, aux)
+    L = cholesky_metric(eng.metric())
+    BQ = whiten_3c2e(eng.int3c("Qmn"), L, layout="Qmn")
+    B = BQ.permute(1, 2, 0).contiguous()
+    barL = torch.as_tensor(O.bar_B_rhf(B.cpu().numpy(), g["D"]), device="cuda")
+    ctx = DFGradContractionContext.build(ao, aux, atom_coords_bohr=g["coords_bohr"], L_chol=L)
+    ref = g["grad_2e"]
+    assert np.abs(ctx.contract(B_ao=B, bar_L_ao=barL) - ref).max() < 1e-9
+    assert np.abs(ctx.contract(B_ao=pack_B_to_Qp(BQ), bar_L_ao=pack_B_to_Qp(barL)) - ref).max() < 1e-9
+    half = 0.5 * barL
+    assert np.abs(ctx.contract_fused_terms(B_ao=B, bar_L_terms=[half, half]) - ref).max() < 1e-9
+    # spherical: with B_sph = T^T B T and bar_L_cart = T bar_L_sph T^T both routes see the same energy
+    T = cart2sph_ao_matrix(ao.shell_l, "cuda")
+    Bs = torch.einsum("ms,nt,mnQ->stQ", T, T, B).contiguous()
+    gen = torch.Generator(device="cuda").manual_seed(0)
+    bar_s = torch.randn((BQ.shape[0], T.shape[1], T.shape[1]), generator=gen, dtype=torch.float64, device="cuda")
+    bar_s = 0.5 * (bar_s + bar_s.transpose(1, 2))
+    bar_c = torch.einsum("ms,Qst,nt->Qmn", T, bar_s, T)
+    g_s = ctx.contract_sph(B_sph=Bs, bar_L_sph=bar_s)
+    g_c = ctx.contract(B_ao=B, bar_L_ao=bar_c)
+    assert np.abs(g_s - g_c).max() < 1e-9 * max(1.0, np.abs(g_c).max())
