@@ -228,6 +228,140 @@ def rhf_df(S, hcore, B=None, *, nelec: int, enuc: float = 0.0, max_cycle: int = 
                      e_elec=float(e_last) - float(enuc), e_nuc=float(enuc), mo_energy=eps, mo_coeff=C, mo_occ=occ)
 
 
+def uhf_df(S, hcore, B=None, *, nalpha: int, nbeta: int, enuc: float = 0.0, max_cycle: int = 50,
+           conv_tol: float = 1e-10, conv_tol_dm: float = 1e-8, diis: bool = True, diis_start_cycle: int = 2,
+           diis_space: int = 8, damping: float = 0.0, jk_mode: str = "auto", k_q_block: int = 128,
+           ao_basis=None, aux_basis=None, df_aux_block_naux: int = 256, L_metric=None, dm0=None,
+           mo_coeff0=None, profile: dict | None = None, engine: DFEngine | None = None, **_unused) -> SCFResult:
+    """UHF with DF J/K (``asuka/hf/df_scf.py:1432-1868`` without the XC terms).
+
+    J comes from the total density and one K per spin from that spin's occupied orbitals
+    (unit occupations); with ``jk_mode='streamed'`` (or 'auto' without B) both spins share
+    one streamed integral evaluation per pass (``df_JKs_streamed``).  Guess, DIIS per spin
+    (from cycle ``diis_start_cycle``), damping, the energy
+    tr(D h) + 1/2 tr(D J) - 1/2 (tr(Da Ka) + tr(Db Kb)) with the new densities and the
+    current J/K, and the convergence test |dE| < conv_tol and
+    ||dDa|| + ||dDb|| < conv_tol_dm follow the reference.
+    """
+    dev = torch.device("cuda", torch.cuda.current_device())
+    S = torch.as_tensor(S, dtype=torch.float64, device=dev)
+    h = torch.as_tensor(hcore, dtype=torch.float64, device=dev)
+    nao = S.shape[0]
+    nalpha, nbeta = int(nalpha), int(nbeta)
+    if nalpha < 0 or nbeta < 0 or nalpha > nao or nbeta > nao:
+        raise ValueError("nalpha/nbeta must lie in [0, nao]")
+    mode = str(jk_mode).strip().lower()
+    streamed = mode == "streamed" or (mode == "auto" and B is None)
+    if streamed:
+        if dm0 is not None:
+            raise NotImplementedError("streamed J/K needs orbitals, not a density guess (dm0)")
+        from .df import get_engine
+        from .streamed import df_JKs_streamed, make_streamed_df_jk_context
+
+        if engine is None and (ao_basis is None or aux_basis is None):
+            raise ValueError("jk_mode='streamed' requires ao_basis and aux_basis")
+        eng = engine if engine is not None else get_engine(ao_basis, aux_basis)
+        ctx = make_streamed_df_jk_context(ao_basis, aux_basis, aux_block_naux=df_aux_block_naux, engine=eng,
+                                          L_metric=None if L_metric is None else torch.as_tensor(L_metric, device=dev))
+    else:
+        if B is None:
+            raise ValueError("B is required unless jk_mode='streamed'")
+        B = torch.as_tensor(B, dtype=torch.float64, device=dev)
+        if B.shape[0] == nao and B.shape[1] == nao:
+            BQ = B.permute(2, 0, 1).contiguous()
+        elif B.shape[1] == nao and B.shape[2] == nao:
+            BQ = B
+        else:
+            raise ValueError("B must be (nao,nao,naux) or (naux,nao,nao)")
+    s, U = torch.linalg.eigh(_sym(S))
+    if bool((s <= 1e-12).any()):
+        raise ValueError("S is not positive definite")
+    Xo = (U * s.rsqrt()) @ U.T
+    occ_a = torch.zeros(nao, dtype=torch.float64, device=dev)
+    occ_b = torch.zeros(nao, dtype=torch.float64, device=dev)
+    occ_a[:nalpha] = 1.0
+    occ_b[:nbeta] = 1.0
+
+    def solve(F):
+        e, Cp = torch.linalg.eigh(_sym(Xo.T @ F @ Xo))
+        return e, Xo @ Cp
+
+    def dens(C, n):
+        Co = C[:, :n]
+        return _sym(Co @ Co.T)
+
+    e0, C = solve(h)
+    Ca = Cb = C
+    ea = eb = e0
+    if dm0 is not None:
+        Da = _sym(torch.as_tensor(dm0[0], dtype=torch.float64, device=dev))
+        Db = _sym(torch.as_tensor(dm0[1], dtype=torch.float64, device=dev))
+    else:
+        if mo_coeff0 is not None:
+            if isinstance(mo_coeff0, (tuple, list)):
+                Ca = torch.as_tensor(mo_coeff0[0], dtype=torch.float64, device=dev)
+                Cb = torch.as_tensor(mo_coeff0[1], dtype=torch.float64, device=dev)
+            else:
+                Ca = Cb = torch.as_tensor(mo_coeff0, dtype=torch.float64, device=dev)
+        Da, Db = dens(Ca, nalpha), dens(Cb, nbeta)
+    lam = float(damping) if damping else 0.0
+    Ka_prev = Kb_prev = None
+    dda = _DIIS(diis_space) if diis else None
+    ddb = _DIIS(diis_space) if diis else None
+    e_last = None
+    converged = False
+    niter = 0
+    for cycle in range(1, max_cycle + 1):
+        niter = cycle
+        Dt = Da + Db
+        if streamed:
+            J, (Ka, Kb) = df_JKs_streamed(ctx, Dt, [Ca[:, :nalpha], Cb[:, :nbeta]],
+                                          [occ_a[:nalpha], occ_b[:nbeta]], k_q_block=k_q_block)
+        elif dm0 is not None and cycle == 1:  # density-driven exchange for a density guess
+            J = df_J_from_BQ_D(BQ, Dt)
+            Ka = _sym(torch.einsum("Qmk,kl,Qnl->mn", BQ, Da, BQ))
+            Kb = _sym(torch.einsum("Qmk,kl,Qnl->mn", BQ, Db, BQ))
+        else:
+            J = df_J_from_BQ_D(BQ, Dt)
+            Ka = df_K_from_BQ_Cw(BQ, Ca[:, :nalpha].contiguous(), q_block=k_q_block)
+            Kb = df_K_from_BQ_Cw(BQ, Cb[:, :nbeta].contiguous(), q_block=k_q_block)
+        if lam and Ka_prev is not None:
+            Ka = (1.0 - lam) * Ka + lam * Ka_prev
+            Kb = (1.0 - lam) * Kb + lam * Kb_prev
+        Ka_prev, Kb_prev = Ka, Kb
+        Fa = _sym(h + J - Ka)
+        Fb = _sym(h + J - Kb)
+        if dda is not None and cycle >= diis_start_cycle:
+            Ma = Fa @ Da @ S
+            dda.push(Fa, Ma - Ma.T)
+            Fa = _sym(dda.extrapolate())
+            Mb = Fb @ Db @ S
+            ddb.push(Fb, Mb - Mb.T)
+            Fb = _sym(ddb.extrapolate())
+        ea, Ca = solve(Fa)
+        eb, Cb = solve(Fb)
+        Da_new, Db_new = dens(Ca, nalpha), dens(Cb, nbeta)
+        if lam:
+            Da_new = (1.0 - lam) * Da_new + lam * Da
+            Db_new = (1.0 - lam) * Db_new + lam * Db
+        Dt_new = Da_new + Db_new
+        e_elec = (float(torch.sum(Dt_new * h)) + 0.5 * float(torch.sum(Dt_new * J))
+                  - 0.5 * (float(torch.sum(Da_new * Ka)) + float(torch.sum(Db_new * Kb))))
+        e_tot = e_elec + float(enuc)
+        dm_err = float(torch.linalg.norm(Da_new - Da)) + float(torch.linalg.norm(Db_new - Db))
+        de = abs(e_tot - e_last) if e_last is not None else float("inf")
+        Da, Db = Da_new, Db_new
+        e_last = e_tot
+        if de < conv_tol and dm_err < conv_tol_dm:
+            converged = True
+            break
+    if profile is not None:
+        profile.setdefault("scf", {}).update(iters=niter)
+    return SCFResult(method="UHF", converged=converged, niter=niter, e_tot=float(e_last),
+                     e_elec=float(e_last) - float(enuc), e_nuc=float(enuc), mo_energy=(ea, eb), mo_coeff=(Ca, Cb),
+                     mo_occ=(occ_a, occ_b))
+
+
 def pack_B_to_Qp(B: torch.Tensor, layout: str = "Qmn") -> torch.Tensor:
     """Lower-triangle packing B_Qp[Q, mu(mu+1)/2 + nu], mu >= nu (``asuka/integrals/df_packed_s2.py:63``)."""
     BQ = B if layout == "Qmn" else B.permute(2, 0, 1)
@@ -255,9 +389,10 @@ def run_hf_df(mol: Molecule, *, method: str = "rhf", backend: str = "cuda", df: 
               conv_tol: float = 1e-10, conv_tol_dm: float = 1e-8, max_cycle: int = 50, precision: str = "fp64",
               df_layout: str = "Qp", df_aux_block_naux: int = 256, profile: dict | None = None,
               **kwargs) -> RHFDFRunResult:
-    """RHF with density fitting on the GPU (``asuka/frontend/scf.py:1219`` for method='rhf')."""
-    if str(method).lower() != "rhf":
-        raise NotImplementedError("only method='rhf' is implemented")
+    """RHF or UHF with density fitting on the GPU (``asuka/frontend/scf.py:1219``)."""
+    meth = str(method).lower()
+    if meth not in ("rhf", "uhf"):
+        raise NotImplementedError("method must be 'rhf' or 'uhf'")
     if backend not in ("cuda", "gpu"):
         raise ValueError("this engine runs on CUDA only (backend='cuda')")
     tb = two_e_backend or ("df" if df else "dense")
@@ -265,8 +400,10 @@ def run_hf_df(mol: Molecule, *, method: str = "rhf", backend: str = "cuda", df: 
         raise NotImplementedError(f"two_e_backend={tb!r} is not implemented")
     if str(auxbasis).lower() not in ("ricd", "accd", "acd"):
         raise NotImplementedError("only the RICD acCD auxiliary basis is available")
-    if mol.spin != 0:
-        raise NotImplementedError("RHF requires spin=0")
+    if meth == "rhf" and mol.spin != 0:
+        raise NotImplementedError("RHF requires spin=0 (use method='uhf')")
+    if (mol.nelectron + mol.spin) % 2:
+        raise ValueError("nelectron and spin are incompatible")
     basis = mol.basis or "ma-svp"
     atoms = list(mol.atoms_bohr)
     ao = bm.pack_basis(atoms, basis, "ao")
@@ -277,6 +414,24 @@ def run_hf_df(mol: Molecule, *, method: str = "rhf", backend: str = "cuda", df: 
     V = eng.metric()
     L = cholesky_metric(V)
     prof = profile if profile is not None else None
+    if meth == "uhf":
+        na, nb = (mol.nelectron + mol.spin) // 2, (mol.nelectron - mol.spin) // 2
+        common = dict(nalpha=na, nbeta=nb, enuc=mol.energy_nuc(), max_cycle=max_cycle, conv_tol=conv_tol,
+                      conv_tol_dm=conv_tol_dm, dm0=dm0, mo_coeff0=mo_coeff0, profile=prof)
+        if tb == "df":
+            B = eng.int3c("Qmn")
+            whiten_3c2e(B, L, layout="Qmn")
+            scf = uhf_df(int1e.S, int1e.hcore, B, jk_mode="materialized", **common)
+            df_B = pack_B_to_Qp(B, "Qmn") if df_layout == "Qp" else (
+                B.permute(1, 2, 0).contiguous() if df_layout == "mnQ" else B)
+        else:
+            scf = uhf_df(int1e.S, int1e.hcore, None, jk_mode="streamed", engine=eng, L_metric=L,
+                         df_aux_block_naux=df_aux_block_naux, **common)
+            df_B = None
+        if prof is not None:
+            prof["wall_s"] = time.perf_counter() - t0
+        return RHFDFRunResult(mol=mol, ao_basis=ao, aux_basis=aux, int1e=int1e, df_B=df_B, df_L=L, scf=scf,
+                              two_e_backend=tb, basis_name=basis, profile=prof)
     if tb == "df":
         B = eng.int3c("Qmn")
         whiten_3c2e(B, L, layout="Qmn")

@@ -18,6 +18,10 @@ Every fixture is produced by the reference's own public CPU path:
 * ``_eri_rys_cpu.eri_rys_tile_cart_sp_batch_cy`` for single (ab|P) and (P|Q)
   tiles of every angular class of H2O/ma-QZVP;
 * ``_eri_rys_cpu.rys_roots_weights_cy`` for reference roots/weights;
+* ``run_hf_df(mol, method='uhf', backend='cpu', df=True, auxbasis='ricd')`` for
+  the open-shell cases (converged energies and orbital energies; the
+  reference's UHF needs a few hundred cycles from the core guess here, hence
+  max_cycle=300);
 * ``asuka.cueri.sph.cart2sph_matrix`` (``asuka/cueri/sph.py:95``) for the
   Cartesian-to-spherical transforms of l = 0..5 (pure Python; importable
   straight from the source tree).
@@ -167,6 +171,22 @@ def roots_case() -> None:
     print("ref_roots: done", flush=True)
 
 
+def uhf_case(name: str, atoms_bohr, basis: str, charge: int, spin: int) -> None:
+    """Open-shell DF-UHF through the reference's CPU path (``run_hf_df(method='uhf', backend='cpu')``)."""
+    from asuka.frontend.molecule import Molecule
+    from asuka.frontend.scf import run_hf_df
+
+    rmol = Molecule.from_atoms([(el, xyz) for el, xyz in atoms_bohr], unit="Bohr", basis=basis, cart=True,
+                               charge=charge, spin=spin)
+    res = run_hf_df(rmol, method="uhf", backend="cpu", df=True, auxbasis="ricd", conv_tol=1e-10, max_cycle=300)
+    ea, eb = (np.asarray(x) for x in res.scf.mo_energy)
+    np.savez_compressed(os.path.join(HERE, f"{name}.npz"), elements=np.array([a for a, _ in atoms_bohr]),
+                        coords_bohr=np.array([x for _, x in atoms_bohr], dtype=np.float64), basis=np.array(basis),
+                        charge=np.array(charge), spin=np.array(spin), e_tot=np.array(res.e_tot),
+                        converged=np.array(bool(res.scf.converged)), niter=np.array(res.scf.niter),
+                        mo_energy_a=ea, mo_energy_b=eb)
+
+
 def sph_case() -> None:
     from asuka.cueri.sph import cart2sph_matrix
 
@@ -181,6 +201,10 @@ CASES = {
     "tiles_h2o_maqzvp": lambda: tiles_case("tiles_h2o_maqzvp", geo.water("ma-qzvp")),
     "ref_roots": roots_case,
     "cart2sph_ref": sph_case,
+    # OH radical (doublet), O-H 0.9697 A along z, and H2O+ (doublet cation) at the water geometry
+    "uhf_oh_masvp": lambda: uhf_case("uhf_oh_masvp", [("O", (0.0, 0.0, 0.0)), ("H", (0.0, 0.0, 0.9697 * geo.ANGSTROM_TO_BOHR))],
+                                     "ma-svp", 0, 1),
+    "uhf_h2o_cation_masvp": lambda: uhf_case("uhf_h2o_cation_masvp", list(geo.water("ma-svp").atoms_bohr), "ma-svp", 1, 1),
 }
 
 if __name__ == "__main__":
