@@ -21,11 +21,11 @@ int dfb_cls_d1_launch(int la, int lb, int lc, const TmplArgs& g, long nblk, size
         return 1;
     }
     if (lb == 0 && lc == 4) {
-        k_rys_thread<1, 0, 4, 8, true, false, 1><<<dim3((unsigned)nblk, 8), 128, smem, st>>>(g);
+        k_rys_thread<1, 0, 4, 8, true, false, 4><<<dim3((unsigned)nblk, 8), 128, smem, st>>>(g);
         return 1;
     }
     if (lb == 0 && lc == 5) {
-        k_rys_thread<1, 0, 5, 11, true, false, 1><<<dim3((unsigned)nblk, 11), 128, smem, st>>>(g);
+        k_rys_thread<1, 0, 5, 11, true, false, 4><<<dim3((unsigned)nblk, 11), 128, smem, st>>>(g);
         return 1;
     }
     if (lb == 0 && lc == 6) {
