@@ -171,20 +171,34 @@ def roots_case() -> None:
     print("ref_roots: done", flush=True)
 
 
-def uhf_case(name: str, atoms_bohr, basis: str, charge: int, spin: int) -> None:
-    """Open-shell DF-UHF through the reference's CPU path (``run_hf_df(method='uhf', backend='cpu')``)."""
+def uhf_case(name: str, atoms_bohr, basis: str, charge: int, spin: int, method: str = "uhf") -> None:
+    """Open-shell DF-UHF/ROHF through the reference's CPU path (``run_hf_df(method=..., backend='cpu')``)."""
     from asuka.frontend.molecule import Molecule
     from asuka.frontend.scf import run_hf_df
 
     rmol = Molecule.from_atoms([(el, xyz) for el, xyz in atoms_bohr], unit="Bohr", basis=basis, cart=True,
                                charge=charge, spin=spin)
-    res = run_hf_df(rmol, method="uhf", backend="cpu", df=True, auxbasis="ricd", conv_tol=1e-10, max_cycle=300)
-    ea, eb = (np.asarray(x) for x in res.scf.mo_energy)
+    res = run_hf_df(rmol, method=method, backend="cpu", df=True, auxbasis="ricd", conv_tol=1e-10, max_cycle=300)
+    me = res.scf.mo_energy
+    ea, eb = (np.asarray(x) for x in me) if isinstance(me, (tuple, list)) else (np.asarray(me), np.asarray(me))
     np.savez_compressed(os.path.join(HERE, f"{name}.npz"), elements=np.array([a for a, _ in atoms_bohr]),
                         coords_bohr=np.array([x for _, x in atoms_bohr], dtype=np.float64), basis=np.array(basis),
                         charge=np.array(charge), spin=np.array(spin), e_tot=np.array(res.e_tot),
                         converged=np.array(bool(res.scf.converged)), niter=np.array(res.scf.niter),
                         mo_energy_a=ea, mo_energy_b=eb)
+
+
+def sph_scf_case(name: str, mol) -> None:
+    """RHF with spherical AOs (``cart=False``) through the reference's CPU path."""
+    from asuka.frontend.molecule import Molecule
+    from asuka.frontend.scf import run_hf_df
+
+    rmol = Molecule.from_atoms([(el, xyz) for el, xyz in mol.atoms_bohr], unit="Bohr", basis=mol.basis, cart=False)
+    res = run_hf_df(rmol, method="rhf", backend="cpu", df=True, auxbasis="ricd", conv_tol=1e-10)
+    np.savez_compressed(os.path.join(HERE, f"{name}.npz"), elements=np.array(mol.elements),
+                        coords_bohr=mol.coords_bohr, basis=np.array(mol.basis), e_tot=np.array(res.e_tot),
+                        niter=np.array(res.scf.niter), mo_energy=np.asarray(res.scf.mo_energy),
+                        S=np.asarray(res.int1e.S), nao=np.array(np.asarray(res.int1e.S).shape[0]))
 
 
 def sph_case() -> None:
@@ -201,9 +215,14 @@ CASES = {
     "tiles_h2o_maqzvp": lambda: tiles_case("tiles_h2o_maqzvp", geo.water("ma-qzvp")),
     "ref_roots": roots_case,
     "cart2sph_ref": sph_case,
+    "sph_h2o_matzvp": lambda: sph_scf_case("sph_h2o_matzvp", geo.water("ma-tzvp")),
     # OH radical (doublet), O-H 0.9697 A along z, and H2O+ (doublet cation) at the water geometry
     "uhf_oh_masvp": lambda: uhf_case("uhf_oh_masvp", [("O", (0.0, 0.0, 0.0)), ("H", (0.0, 0.0, 0.9697 * geo.ANGSTROM_TO_BOHR))],
                                      "ma-svp", 0, 1),
+    "rohf_oh_masvp": lambda: uhf_case("rohf_oh_masvp", [("O", (0.0, 0.0, 0.0)), ("H", (0.0, 0.0, 0.9697 * geo.ANGSTROM_TO_BOHR))],
+                                      "ma-svp", 0, 1, "rohf"),
+    "rohf_h2o_cation_masvp": lambda: uhf_case("rohf_h2o_cation_masvp", list(geo.water("ma-svp").atoms_bohr), "ma-svp", 1,
+                                              1, "rohf"),
     "uhf_h2o_cation_masvp": lambda: uhf_case("uhf_h2o_cation_masvp", list(geo.water("ma-svp").atoms_bohr), "ma-svp", 1, 1),
 }
 
