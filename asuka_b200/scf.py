@@ -362,6 +362,145 @@ def uhf_df(S, hcore, B=None, *, nalpha: int, nbeta: int, enuc: float = 0.0, max_
                      mo_occ=(occ_a, occ_b))
 
 
+def _roothaan_fock(Fa, Fb, Da, Db, S):
+    """Roothaan's effective ROHF Fock matrix from the spin Fock matrices.
+
+    With the closed (c), open (o) and virtual (v) projectors P_c = Db S, P_o = (Da - Db) S,
+    P_v = 1 - Da S and Fc = (Fa + Fb)/2, the blocks are cc, oo, vv: Fc; oc: Fb; ov: Fa;
+    vc: Fc (the choice of ``asuka/hf/df_scf.py:691-719``, as in PySCF's get_roothaan_fock).
+    """
+    n = S.shape[0]
+    fc = 0.5 * (Fa + Fb)
+    pc = Db @ S
+    po = (Da - Db) @ S
+    pv = torch.eye(n, dtype=S.dtype, device=S.device) - Da @ S
+    F = 0.5 * (pc.T @ fc @ pc + po.T @ fc @ po + pv.T @ fc @ pv)
+    F = F + po.T @ Fb @ pc + po.T @ Fa @ pv + pv.T @ fc @ pc
+    return _sym(F + F.T)
+
+
+def rohf_df(S, hcore, B=None, *, nalpha: int, nbeta: int, enuc: float = 0.0, max_cycle: int = 50,
+            conv_tol: float = 1e-10, conv_tol_dm: float = 1e-8, diis: bool = True, diis_start_cycle: int = 2,
+            diis_space: int = 8, damping: float = 0.0, jk_mode: str = "auto", k_q_block: int = 128,
+            ao_basis=None, aux_basis=None, df_aux_block_naux: int = 256, L_metric=None, dm0=None,
+            mo_coeff0=None, profile: dict | None = None, engine: DFEngine | None = None, **_unused) -> SCFResult:
+    """ROHF with DF J/K and one set of orbitals (``asuka/hf/df_scf.py:1870-2330``).
+
+    Spin Fock matrices Fa = h + J - Ka, Fb = h + J - Kb are combined into Roothaan's
+    effective Fock (``_roothaan_fock``); DIIS runs on it with the error F Dt S - S Dt F.
+    With streamed J/K the beta orbitals and the open shell go through one integral pass
+    as two occupied sets (Ka = Kb + K_open).  Energy and convergence test as for UHF.
+    """
+    dev = torch.device("cuda", torch.cuda.current_device())
+    S = torch.as_tensor(S, dtype=torch.float64, device=dev)
+    h = torch.as_tensor(hcore, dtype=torch.float64, device=dev)
+    nao = S.shape[0]
+    nalpha, nbeta = int(nalpha), int(nbeta)
+    if not (0 <= nbeta <= nalpha <= nao):
+        raise ValueError("ROHF needs 0 <= nbeta <= nalpha <= nao")
+    mode = str(jk_mode).strip().lower()
+    streamed = mode == "streamed" or (mode == "auto" and B is None)
+    if streamed:
+        if dm0 is not None:
+            raise NotImplementedError("streamed J/K needs orbitals, not a density guess (dm0)")
+        from .df import get_engine
+        from .streamed import df_JKs_streamed, make_streamed_df_jk_context
+
+        if engine is None and (ao_basis is None or aux_basis is None):
+            raise ValueError("jk_mode='streamed' requires ao_basis and aux_basis")
+        eng = engine if engine is not None else get_engine(ao_basis, aux_basis)
+        ctx = make_streamed_df_jk_context(ao_basis, aux_basis, aux_block_naux=df_aux_block_naux, engine=eng,
+                                          L_metric=None if L_metric is None else torch.as_tensor(L_metric, device=dev))
+    else:
+        if B is None:
+            raise ValueError("B is required unless jk_mode='streamed'")
+        B = torch.as_tensor(B, dtype=torch.float64, device=dev)
+        if B.shape[0] == nao and B.shape[1] == nao:
+            BQ = B.permute(2, 0, 1).contiguous()
+        elif B.shape[1] == nao and B.shape[2] == nao:
+            BQ = B
+        else:
+            raise ValueError("B must be (nao,nao,naux) or (naux,nao,nao)")
+    s, U = torch.linalg.eigh(_sym(S))
+    if bool((s <= 1e-12).any()):
+        raise ValueError("S is not positive definite")
+    Xo = (U * s.rsqrt()) @ U.T
+    occ_a = torch.zeros(nao, dtype=torch.float64, device=dev)
+    occ_b = torch.zeros(nao, dtype=torch.float64, device=dev)
+    occ_a[:nalpha] = 1.0
+    occ_b[:nbeta] = 1.0
+
+    def solve(F):
+        e, Cp = torch.linalg.eigh(_sym(Xo.T @ F @ Xo))
+        return e, Xo @ Cp
+
+    def dens(C, n):
+        Co = C[:, :n]
+        return _sym(Co @ Co.T)
+
+    eps, C = solve(h)
+    if dm0 is not None:
+        Da = _sym(torch.as_tensor(dm0[0], dtype=torch.float64, device=dev))
+        Db = _sym(torch.as_tensor(dm0[1], dtype=torch.float64, device=dev))
+    else:
+        if mo_coeff0 is not None:
+            C = torch.as_tensor(mo_coeff0, dtype=torch.float64, device=dev)
+        Da, Db = dens(C, nalpha), dens(C, nbeta)
+    lam = float(damping) if damping else 0.0
+    Ka_prev = Kb_prev = None
+    dd = _DIIS(diis_space) if diis else None
+    e_last = None
+    converged = False
+    niter = 0
+    for cycle in range(1, max_cycle + 1):
+        niter = cycle
+        Dt = Da + Db
+        if streamed:
+            J, (Kb, Ko) = df_JKs_streamed(ctx, Dt, [C[:, :nbeta], C[:, nbeta:nalpha]],
+                                          [occ_b[:nbeta], occ_a[nbeta:nalpha]], k_q_block=k_q_block)
+            Ka = Kb + Ko
+        elif dm0 is not None and cycle == 1:
+            J = df_J_from_BQ_D(BQ, Dt)
+            Ka = _sym(torch.einsum("Qmk,kl,Qnl->mn", BQ, Da, BQ))
+            Kb = _sym(torch.einsum("Qmk,kl,Qnl->mn", BQ, Db, BQ))
+        else:
+            J = df_J_from_BQ_D(BQ, Dt)
+            Ka = df_K_from_BQ_Cw(BQ, C[:, :nalpha].contiguous(), q_block=k_q_block)
+            Kb = df_K_from_BQ_Cw(BQ, C[:, :nbeta].contiguous(), q_block=k_q_block)
+        if lam and Ka_prev is not None:
+            Ka = (1.0 - lam) * Ka + lam * Ka_prev
+            Kb = (1.0 - lam) * Kb + lam * Kb_prev
+        Ka_prev, Kb_prev = Ka, Kb
+        Fa = _sym(h + J - Ka)
+        Fb = _sym(h + J - Kb)
+        F = _roothaan_fock(Fa, Fb, Da, Db, S)
+        if dd is not None and cycle >= diis_start_cycle:
+            M = F @ Dt @ S
+            dd.push(F, M - M.T)
+            F = _sym(dd.extrapolate())
+        eps, C = solve(F)
+        Da_new, Db_new = dens(C, nalpha), dens(C, nbeta)
+        if lam:
+            Da_new = (1.0 - lam) * Da_new + lam * Da
+            Db_new = (1.0 - lam) * Db_new + lam * Db
+        Dt_new = Da_new + Db_new
+        e_elec = (float(torch.sum(Dt_new * h)) + 0.5 * float(torch.sum(Dt_new * J))
+                  - 0.5 * (float(torch.sum(Da_new * Ka)) + float(torch.sum(Db_new * Kb))))
+        e_tot = e_elec + float(enuc)
+        dm_err = float(torch.linalg.norm(Da_new - Da)) + float(torch.linalg.norm(Db_new - Db))
+        de = abs(e_tot - e_last) if e_last is not None else float("inf")
+        Da, Db = Da_new, Db_new
+        e_last = e_tot
+        if de < conv_tol and dm_err < conv_tol_dm:
+            converged = True
+            break
+    if profile is not None:
+        profile.setdefault("scf", {}).update(iters=niter)
+    return SCFResult(method="ROHF", converged=converged, niter=niter, e_tot=float(e_last),
+                     e_elec=float(e_last) - float(enuc), e_nuc=float(enuc), mo_energy=eps, mo_coeff=C,
+                     mo_occ=(occ_a, occ_b))
+
+
 def pack_B_to_Qp(B: torch.Tensor, layout: str = "Qmn") -> torch.Tensor:
     """Lower-triangle packing B_Qp[Q, mu(mu+1)/2 + nu], mu >= nu (``asuka/integrals/df_packed_s2.py:63``)."""
     BQ = B if layout == "Qmn" else B.permute(2, 0, 1)
@@ -391,8 +530,8 @@ def run_hf_df(mol: Molecule, *, method: str = "rhf", backend: str = "cuda", df: 
               **kwargs) -> RHFDFRunResult:
     """RHF or UHF with density fitting on the GPU (``asuka/frontend/scf.py:1219``)."""
     meth = str(method).lower()
-    if meth not in ("rhf", "uhf"):
-        raise NotImplementedError("method must be 'rhf' or 'uhf'")
+    if meth not in ("rhf", "uhf", "rohf"):
+        raise NotImplementedError("method must be 'rhf', 'uhf' or 'rohf'")
     if backend not in ("cuda", "gpu"):
         raise ValueError("this engine runs on CUDA only (backend='cuda')")
     tb = two_e_backend or ("df" if df else "dense")
@@ -414,18 +553,36 @@ def run_hf_df(mol: Molecule, *, method: str = "rhf", backend: str = "cuda", df: 
     V = eng.metric()
     L = cholesky_metric(V)
     prof = profile if profile is not None else None
-    if meth == "uhf":
+    Tsph = None
+    if not getattr(mol, "cart", True):
+        # spherical AOs: the integrals are evaluated over Cartesian shells and transformed on the
+        # AO indices (X_sph = T^T X T, the aux index stays Cartesian), as the reference does
+        from .int1e import Int1eResult
+        from .sph import cart2sph_ao_matrix, int3c_cart_to_sph
+
+        Tsph = cart2sph_ao_matrix(ao.shell_l, eng.device)
+        Tn = Tsph.cpu().numpy()
+        int1e = Int1eResult(S=Tn.T @ int1e.S @ Tn, T=Tn.T @ int1e.T @ Tn, V=Tn.T @ int1e.V @ Tn)
+        if tb == "direct_df" and meth != "rhf":
+            raise NotImplementedError("streamed J/K with spherical AOs is implemented for RHF only")
+
+    def _B_for_scf():
+        B = eng.int3c("Qmn")
+        whiten_3c2e(B, L, layout="Qmn")
+        return B if Tsph is None else int3c_cart_to_sph(B, Tsph, "Qmn")
+
+    if meth in ("uhf", "rohf"):
+        driver = uhf_df if meth == "uhf" else rohf_df
         na, nb = (mol.nelectron + mol.spin) // 2, (mol.nelectron - mol.spin) // 2
         common = dict(nalpha=na, nbeta=nb, enuc=mol.energy_nuc(), max_cycle=max_cycle, conv_tol=conv_tol,
                       conv_tol_dm=conv_tol_dm, dm0=dm0, mo_coeff0=mo_coeff0, profile=prof)
         if tb == "df":
-            B = eng.int3c("Qmn")
-            whiten_3c2e(B, L, layout="Qmn")
-            scf = uhf_df(int1e.S, int1e.hcore, B, jk_mode="materialized", **common)
+            B = _B_for_scf()
+            scf = driver(int1e.S, int1e.hcore, B, jk_mode="materialized", **common)
             df_B = pack_B_to_Qp(B, "Qmn") if df_layout == "Qp" else (
                 B.permute(1, 2, 0).contiguous() if df_layout == "mnQ" else B)
         else:
-            scf = uhf_df(int1e.S, int1e.hcore, None, jk_mode="streamed", engine=eng, L_metric=L,
+            scf = driver(int1e.S, int1e.hcore, None, jk_mode="streamed", engine=eng, L_metric=L,
                          df_aux_block_naux=df_aux_block_naux, **common)
             df_B = None
         if prof is not None:
@@ -433,8 +590,7 @@ def run_hf_df(mol: Molecule, *, method: str = "rhf", backend: str = "cuda", df: 
         return RHFDFRunResult(mol=mol, ao_basis=ao, aux_basis=aux, int1e=int1e, df_B=df_B, df_L=L, scf=scf,
                               two_e_backend=tb, basis_name=basis, profile=prof)
     if tb == "df":
-        B = eng.int3c("Qmn")
-        whiten_3c2e(B, L, layout="Qmn")
+        B = _B_for_scf()
         scf = rhf_df(int1e.S, int1e.hcore, B, nelec=mol.nelectron, enuc=mol.energy_nuc(), max_cycle=max_cycle,
                      conv_tol=conv_tol, conv_tol_dm=conv_tol_dm, dm0=dm0, mo_coeff0=mo_coeff0, precision=precision,
                      profile=prof)
@@ -446,6 +602,12 @@ def run_hf_df(mol: Molecule, *, method: str = "rhf", backend: str = "cuda", df: 
             df_B = B
     else:
         jk = _direct_jk(eng, L, aux_block=df_aux_block_naux)
+        if Tsph is not None:
+            jk_cart = jk
+
+            def jk(D, Cw, prec, _T=Tsph, _jk=jk_cart):
+                Jc, Kc = _jk(_T @ D @ _T.T, _T @ Cw, prec)
+                return _T.T @ Jc @ _T, _T.T @ Kc @ _T
         scf = rhf_df(int1e.S, int1e.hcore, None, nelec=mol.nelectron, enuc=mol.energy_nuc(), max_cycle=max_cycle,
                      conv_tol=conv_tol, conv_tol_dm=conv_tol_dm, dm0=dm0, mo_coeff0=mo_coeff0, precision="fp64",
                      jk_fn=jk, profile=prof)
