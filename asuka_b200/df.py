@@ -494,6 +494,68 @@ class DFEngine:
         return grad
 
 
+    # ------------------------------------------------------------ overlapped phases of one step
+    def metric_cholesky_int3c(self, X: torch.Tensor | None = None):
+        """V = (P|Q), its Cholesky factor L and X = (mu nu|P) ('Qmn') with the phases overlapped.
+
+        The metric classes go to the side streams first and the 3c classes after them; the
+        main stream waits only for the metric launches, symmetrizes V and factorises it while
+        the 3c classes still run, then joins.  Same results as metric(), cholesky_metric() and
+        int3c() in sequence.
+        """
+        nao, naux = self.nao, self.naux
+        if NSTREAMS <= 1:
+            V = self.metric()
+            return V, cholesky_metric(V), self.int3c("Qmn", out=X)
+        V = torch.empty((naux, naux), dtype=torch.float64, device=self.device)
+        X = X if X is not None else torch.empty((naux, nao, nao), dtype=torch.float64, device=self.device)
+        if self.n_dropped_pairs:
+            X.zero_()
+        self._slices_int = self._scratch_slices(False)
+        first = [self._launch_int(lp, 0, lq, self.ps_aux, self.axs, P, Q, P.numel(), 0, 1, V, (naux, 1, 0))
+                 for lp, lq, P, Q in self.classes2c]
+        second = [self._launch_int(la, lb, lc, self.ps_ao, self.axs, pairs, auxs, pairs.numel() * auxs.numel(),
+                                   -pairs.numel(), 0, X, (nao * nao, nao, 1))
+                  for la, lb, lc, pairs, auxs in self.classes3c]
+        main = torch.cuda.current_stream(self.device)
+        side = self._streams()
+        start = torch.cuda.Event()
+        start.record(main)
+        for st in side:
+            st.wait_event(start)
+        for i, fn in enumerate(first):
+            fn(int(side[i % len(side)].cuda_stream))
+        for st in side:
+            ev = torch.cuda.Event()
+            ev.record(st)
+            main.wait_event(ev)
+        for i, fn in enumerate(second):
+            fn(int(side[(i + len(first)) % len(side)].cuda_stream))
+        V.copy_(0.5 * (V + V.T))
+        L, info = torch.linalg.cholesky_ex(V)
+        for st in side:
+            ev = torch.cuda.Event()
+            ev.record(st)
+            main.wait_event(ev)
+        if int(info.item()) != 0:
+            raise RuntimeError(f"metric Cholesky failed (leading minor {int(info.item())} not positive definite)")
+        return V, L, X
+
+    def deriv3c_2c(self, bar3: torch.Tensor, bar2: torch.Tensor, grad: torch.Tensor) -> torch.Tensor:
+        """deriv3c(bar3 'Qmn') and deriv2c(bar2) as one fan-out (both add into grad atomically)."""
+        nao, naux = self.nao, self.naux
+        bar3 = bar3.contiguous()
+        bar2 = bar2.contiguous()
+        self._slices_der = self._scratch_slices(True)
+        launches = [self._launch_deriv(la, lb, lc, self.ps_ao, self.axs, pairs, auxs, pairs.numel() * auxs.numel(),
+                                       -pairs.numel(), 0, bar3, (nao * nao, nao, 1), grad)
+                    for la, lb, lc, pairs, auxs in self.classes3c]
+        launches += [self._launch_deriv(lp, 0, lq, self.ps_aux, self.axs, P, Q, P.numel(), 0, 1, bar2, (naux, 1, 0),
+                                        grad) for lp, lq, P, Q in self.classes2c]
+        self._fanout(launches)
+        return grad
+
+
 # ---------------------------------------------------------------- reference seams
 
 _ENGINES: "weakref.WeakValueDictionary" = weakref.WeakValueDictionary()

@@ -44,9 +44,7 @@ def _nomark(_key: str) -> None:
 
 def df_forward(engine: DFEngine, Cw: torch.Tensor, precision: str = "fp64", X: torch.Tensor | None = None):
     """Integrals at the engine's current geometry, then (E_2e, J, K) and the saved intermediates."""
-    V = engine.metric()
-    L = cholesky_metric(V)
-    X = engine.int3c("Qmn", out=X)
+    _V, L, X = engine.metric_cholesky_int3c(X)
     return df_contract(engine, Cw, X, L, precision)
 
 
@@ -109,8 +107,7 @@ def df_backward(engine: DFEngine, Cw: torch.Tensor, saved: dict, grad: torch.Ten
     G3, G2 = df_adjoints(engine, Cw, saved)
     if grad is None:
         grad = torch.zeros((engine.natm, 3), dtype=torch.float64, device=G3.device)
-    engine.deriv3c(G3, grad, layout="Qmn")
-    engine.deriv2c(G2, grad)
+    engine.deriv3c_2c(G3, G2, grad)
     return grad
 
 
