@@ -75,33 +75,51 @@ def build(force: bool = False, verbose: bool = False, jobs: int | None = None) -
     return OUT
 
 
-def build_variant(defines: list[str], out: str, tag: str, jobs: int | None = None) -> str:
-    """A second library whose class-specialised kernels are compiled with extra -D defines
-    (objects in _build_<tag>); the other sources reuse the main build's objects."""
+def build_variant(defines: list[str], out: str, tag: str, jobs: int | None = None,
+                  gen_env: dict | None = None) -> str:
+    """A second library for the class tuner (objects in _build_<tag>).
+
+    ``defines``: extra -D flags for the class-specialised kernels, the other sources reuse
+    the main build's objects.  ``gen_env``: regenerate the class kernels under these
+    environment variables (e.g. another accumulator budget) in a copy of csrc and build
+    every source of that copy (the dispatcher depends on the generated class set).
+    """
+    import shutil
+
     build()
     nvcc = os.environ.get("NVCC", "nvcc")
     objdir = os.path.join(HERE, "_build")
     vdir = os.path.join(HERE, f"_build_{tag}")
     os.makedirs(vdir, exist_ok=True)
     compile_flags = [f for f in NVCC_FLAGS if f not in ("--shared", "-lcublas")] + [f"-D{d}" for d in defines]
+    # the sources include "../../include/dfb.h" relative to csrc: -I csrc resolves it for the copy too
+    inc = ["-I", CSRC]
+    srcdir = CSRC
+    if gen_env:
+        srcdir = os.path.join(vdir, "src")
+        if os.path.exists(srcdir):
+            shutil.rmtree(srcdir)
+        shutil.copytree(CSRC, srcdir, ignore=shutil.ignore_patterns("class_tuning.json", "__pycache__"))
+        env = dict(os.environ, **gen_env)
+        subprocess.run([sys.executable, os.path.join(srcdir, "gen_classes.py"), srcdir], check=True, env=env)
     objs, procs = [], []
     jobs = jobs or max(1, os.cpu_count() or 1)
-    for src in sources():
+    for src in sorted(glob.glob(os.path.join(srcdir, "*.cu"))):
         base = os.path.basename(src)[:-3]
-        if not base.startswith("dfb_cls_"):
+        if not gen_env and not base.startswith("dfb_cls_"):
             objs.append(os.path.join(objdir, base + ".o"))
             continue
         obj = os.path.join(vdir, base + ".o")
         objs.append(obj)
         while len([p for p in procs if p.poll() is None]) >= jobs:
             procs[0].wait() if procs[0].poll() is None else procs.pop(0)
-        procs.append(subprocess.Popen([nvcc, *compile_flags, "-c", src, "-o", obj], cwd=CSRC))
+        procs.append(subprocess.Popen([nvcc, *compile_flags, *inc, "-c", src, "-o", obj], cwd=srcdir))
     for p in procs:
         if p.wait() != 0:
             raise RuntimeError(f"nvcc failed: {p.args}")
     os.makedirs(os.path.dirname(out), exist_ok=True)
     subprocess.run([nvcc, "-gencode", "arch=compute_100a,code=sm_100a", "--shared", "-o", out, *objs],
-                   check=True, cwd=CSRC)
+                   check=True, cwd=srcdir)
     return out
 
 

@@ -13,23 +13,23 @@ int dfb_cls_d1_launch(int la, int lb, int lc, const TmplArgs& g, long nblk, size
         return 1;
     }
     if (lb == 0 && lc == 2) {
-        k_rys_thread<1, 0, 2, 3, true, false, 1><<<dim3((unsigned)nblk, 3), 128, smem, st>>>(g);
+        k_rys_thread<1, 0, 2, 2, true, false, 1><<<dim3((unsigned)nblk, 2), 128, smem, st>>>(g);
         return 1;
     }
     if (lb == 0 && lc == 3) {
-        k_rys_thread<1, 0, 3, 5, true, false, 1><<<dim3((unsigned)nblk, 5), 128, smem, st>>>(g);
+        k_rys_thread<1, 0, 3, 4, true, false, 1><<<dim3((unsigned)nblk, 4), 128, smem, st>>>(g);
         return 1;
     }
     if (lb == 0 && lc == 4) {
-        k_rys_thread<1, 0, 4, 8, true, false, 4><<<dim3((unsigned)nblk, 8), 128, smem, st>>>(g);
+        k_rys_thread<1, 0, 4, 5, true, false, 1><<<dim3((unsigned)nblk, 5), 128, smem, st>>>(g);
         return 1;
     }
     if (lb == 0 && lc == 5) {
-        k_rys_thread<1, 0, 5, 11, true, false, 4><<<dim3((unsigned)nblk, 11), 128, smem, st>>>(g);
+        k_rys_thread<1, 0, 5, 7, true, false, 1><<<dim3((unsigned)nblk, 7), 128, smem, st>>>(g);
         return 1;
     }
     if (lb == 0 && lc == 6) {
-        k_rys_thread<1, 0, 6, 14, true, false, 1><<<dim3((unsigned)nblk, 14), 128, smem, st>>>(g);
+        k_rys_thread<1, 0, 6, 10, true, false, 1><<<dim3((unsigned)nblk, 10), 128, smem, st>>>(g);
         return 1;
     }
     if (lb == 1 && lc == 0) {

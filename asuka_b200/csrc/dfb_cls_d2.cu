@@ -9,7 +9,7 @@ int dfb_cls_d2_launch(int la, int lb, int lc, const TmplArgs& g, long nblk, size
         return 1;
     }
     if (lb == 0 && lc == 1) {
-        k_rys_thread<2, 0, 1, 3, true, false, 1><<<dim3((unsigned)nblk, 3), 128, smem, st>>>(g);
+        k_rys_thread<2, 0, 1, 3, true, false, 4><<<dim3((unsigned)nblk, 3), 128, smem, st>>>(g);
         return 1;
     }
     if (lb == 0 && lc == 2) {
@@ -37,19 +37,19 @@ int dfb_cls_d2_launch(int la, int lb, int lc, const TmplArgs& g, long nblk, size
         return 1;
     }
     if (lb == 1 && lc == 1) {
-        k_rys_thread<2, 1, 1, 3, true, true, 1><<<dim3((unsigned)nblk, 6), 128, smem, st>>>(g);
+        k_rys_thread<2, 1, 1, 2, true, true, 1><<<dim3((unsigned)nblk, 4), 128, smem, st>>>(g);
         return 1;
     }
     if (lb == 1 && lc == 2) {
-        k_rys_thread<2, 1, 2, 6, true, true, 1><<<dim3((unsigned)nblk, 12), 128, smem, st>>>(g);
+        k_rys_thread<2, 1, 2, 3, true, true, 1><<<dim3((unsigned)nblk, 6), 128, smem, st>>>(g);
         return 1;
     }
     if (lb == 1 && lc == 3) {
-        k_rys_thread<2, 1, 3, 10, true, true, 1><<<dim3((unsigned)nblk, 20), 128, smem, st>>>(g);
+        k_rys_thread<2, 1, 3, 5, true, true, 1><<<dim3((unsigned)nblk, 10), 128, smem, st>>>(g);
         return 1;
     }
     if (lb == 1 && lc == 4) {
-        k_rys_thread<2, 1, 4, 15, true, true, 1><<<dim3((unsigned)nblk, 30), 128, smem, st>>>(g);
+        k_rys_thread<2, 1, 4, 8, true, true, 1><<<dim3((unsigned)nblk, 16), 128, smem, st>>>(g);
         return 1;
     }
     if (lb == 1 && lc == 5) {
@@ -58,6 +58,30 @@ int dfb_cls_d2_launch(int la, int lb, int lc, const TmplArgs& g, long nblk, size
     }
     if (lb == 1 && lc == 6) {
         k_rys_thread<2, 1, 6, 28, true, true, 1><<<dim3((unsigned)nblk, 56), 128, smem, st>>>(g);
+        return 1;
+    }
+    if (lb == 2 && lc == 0) {
+        k_rys_thread<2, 2, 0, 1, true, true, 1><<<dim3((unsigned)nblk, 2), 128, smem, st>>>(g);
+        return 1;
+    }
+    if (lb == 2 && lc == 1) {
+        k_rys_thread<2, 2, 1, 3, true, true, 1><<<dim3((unsigned)nblk, 6), 128, smem, st>>>(g);
+        return 1;
+    }
+    if (lb == 2 && lc == 2) {
+        k_rys_thread<2, 2, 2, 6, true, true, 1><<<dim3((unsigned)nblk, 12), 128, smem, st>>>(g);
+        return 1;
+    }
+    if (lb == 2 && lc == 3) {
+        k_rys_thread<2, 2, 3, 10, true, true, 1><<<dim3((unsigned)nblk, 20), 128, smem, st>>>(g);
+        return 1;
+    }
+    if (lb == 2 && lc == 4) {
+        k_rys_thread<2, 2, 4, 15, true, true, 1><<<dim3((unsigned)nblk, 30), 128, smem, st>>>(g);
+        return 1;
+    }
+    if (lb == 2 && lc == 5) {
+        k_rys_thread<2, 2, 5, 21, true, true, 1><<<dim3((unsigned)nblk, 42), 128, smem, st>>>(g);
         return 1;
     }
     return 0;

@@ -13,7 +13,7 @@ int dfb_cls_d3_launch(int la, int lb, int lc, const TmplArgs& g, long nblk, size
         return 1;
     }
     if (lb == 0 && lc == 2) {
-        k_rys_thread<3, 0, 2, 3, true, true, 1><<<dim3((unsigned)nblk, 6), 128, smem, st>>>(g);
+        k_rys_thread<3, 0, 2, 6, true, false, 1><<<dim3((unsigned)nblk, 6), 128, smem, st>>>(g);
         return 1;
     }
     if (lb == 0 && lc == 3) {
@@ -25,11 +25,11 @@ int dfb_cls_d3_launch(int la, int lb, int lc, const TmplArgs& g, long nblk, size
         return 1;
     }
     if (lb == 0 && lc == 5) {
-        k_rys_thread<3, 0, 5, 21, true, true, 1><<<dim3((unsigned)nblk, 42), 128, smem, st>>>(g);
+        k_rys_thread<3, 0, 5, 21, true, false, 1><<<dim3((unsigned)nblk, 21), 128, smem, st>>>(g);
         return 1;
     }
     if (lb == 0 && lc == 6) {
-        k_rys_thread<3, 0, 6, 28, true, true, 1><<<dim3((unsigned)nblk, 56), 128, smem, st>>>(g);
+        k_rys_thread<3, 0, 6, 28, true, false, 1><<<dim3((unsigned)nblk, 28), 128, smem, st>>>(g);
         return 1;
     }
     if (lb == 1 && lc == 0) {
@@ -54,6 +54,22 @@ int dfb_cls_d3_launch(int la, int lb, int lc, const TmplArgs& g, long nblk, size
     }
     if (lb == 1 && lc == 5) {
         k_rys_thread<3, 1, 5, 21, true, true, 1><<<dim3((unsigned)nblk, 42), 128, smem, st>>>(g);
+        return 1;
+    }
+    if (lb == 2 && lc == 0) {
+        k_rys_thread<3, 2, 0, 1, true, true, 1><<<dim3((unsigned)nblk, 2), 128, smem, st>>>(g);
+        return 1;
+    }
+    if (lb == 2 && lc == 1) {
+        k_rys_thread<3, 2, 1, 3, true, true, 1><<<dim3((unsigned)nblk, 6), 128, smem, st>>>(g);
+        return 1;
+    }
+    if (lb == 2 && lc == 2) {
+        k_rys_thread<3, 2, 2, 6, true, true, 1><<<dim3((unsigned)nblk, 12), 128, smem, st>>>(g);
+        return 1;
+    }
+    if (lb == 2 && lc == 3) {
+        k_rys_thread<3, 2, 3, 10, true, true, 1><<<dim3((unsigned)nblk, 20), 128, smem, st>>>(g);
         return 1;
     }
     return 0;

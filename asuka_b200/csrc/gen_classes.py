@@ -59,8 +59,23 @@ def acc_per_f(la, lb, mode):
     return nrange(la, la + lb - 1) + nrange(la, la + lb + 1)
 
 
-def plan(la, lb, lc, deriv):
-    """(FS, SPLIT) for a class, or None when it stays on the generic warp kernel."""
+def _key(la, lb, lc, deriv):
+    return f"{'d' if deriv else 'i'}{la}{lb}{lc}"
+
+
+def plan(la, lb, lc, deriv, budget=None):
+    """(FS, SPLIT) for a class, or None when it stays on the generic warp kernel.
+
+    ``budget`` overrides the accumulator budget; without it the measured per-class table
+    (``class_tuning.json``, "acc_budget") or the default ACC_BUDGET applies.  The
+    environment variable DFB_GEN_ACC_BUDGET_DERIV sets the derivative default (the tuner's
+    variant builds).
+    """
+    if budget is None:
+        budget = tuning("acc_budget").get(_key(la, lb, lc, deriv))
+    if budget is None:
+        env = os.environ.get("DFB_GEN_ACC_BUDGET_DERIV")
+        budget = int(env) if (env and deriv) else ACC_BUDGET[deriv]
     nm = la + lb + (1 if deriv else 0)
     nf = ncart(lc)
     modes = [(1, False), (None, True)] if deriv else [(0, False)]
@@ -70,20 +85,22 @@ def plan(la, lb, lc, deriv):
             nfs = -(-nf // fs)
             if -(-nf // nfs) != fs:
                 continue  # keep the split exact (no empty subsets)
-            if per_f * nfs <= ACC_BUDGET[deriv] and g_cost(nm, lc, nfs) <= G_BUDGET:
+            if per_f * nfs <= budget and g_cost(nm, lc, nfs) <= G_BUDGET:
                 return fs, split
     return None
 
 
-def tuning() -> dict:
-    """Per-class launch-bounds choices measured by asuka_b200.tune_classes (empty when absent)."""
+def tuning(field: str = "min_blocks") -> dict:
+    """Per-class choices measured by asuka_b200.tune_classes ("min_blocks": launch bounds,
+    "acc_budget": accumulator budget of the component split); empty when absent or when
+    DFB_GEN_NO_TUNING is set (the tuner's variant builds)."""
     import json
 
     p = os.path.join(HERE, "class_tuning.json")
-    if not os.path.exists(p):
+    if os.environ.get("DFB_GEN_NO_TUNING") or not os.path.exists(p):
         return {}
     with open(p) as f:
-        return json.load(f).get("min_blocks", {})
+        return json.load(f).get(field, {})
 
 
 def main() -> None:
@@ -113,7 +130,7 @@ def main() -> None:
                 "    (void)la;",
             ]
             for (a, b, c, fs, split) in cls:
-                minb = int(tune.get(f"{'d' if deriv else 'i'}{a}{b}{c}", 1))
+                minb = int(tune.get(_key(a, b, c, deriv), 1))
                 kern = (f"k_rys_thread<{a}, {b}, {c}, {fs}, {'true' if deriv else 'false'}, "
                         f"{'true' if split else 'false'}, {minb}>")
                 lines.append(f"    if (lb == {b} && lc == {c}) {{")
@@ -152,4 +169,8 @@ def main() -> None:
 
 
 if __name__ == "__main__":
+    import sys
+
+    if len(sys.argv) > 1:  # generate into another directory (the tuner's variant builds)
+        HERE = os.path.abspath(sys.argv[1])
     main()

@@ -1,16 +1,25 @@
-"""Measured per-class launch bounds for the class-specialised Rys kernels.
+"""Measured per-class kernel shapes for the class-specialised Rys kernels (the autotuner).
 
-The thread kernels run 128 threads per block.  By default the compiler may give a
-thread up to 255 registers (the classes take 150-170, i.e. 3 resident blocks per SM);
-capping them at 128 (4 blocks per SM) helps the classes whose working set still fits and
-hurts the ones that then spill.  Which is which is measured, not guessed:
+Two knobs are tuned per angular class, each against the default build:
 
-    python -m asuka_b200.tune_classes build                   # (no GPU) variant library, every class capped
-    python -m asuka_b200.tune_classes measure w8 w4q --out T  # (GPU) time every class with both libraries
+* launch bounds: the thread kernels run 128 threads per block and may take up to 255
+  registers (the classes use 150-170, i.e. 3 resident blocks per SM); capping them at 128
+  (4 blocks per SM) helps the classes whose working set still fits and hurts those that spill
+  (variant "minb4");
+* the aux-component split: a derivative class is split over FS threads per task so that one
+  thread's accumulators fit a register budget; every extra split repeats the task's Rys roots
+  and recurrence tables, a larger budget (fewer, heavier threads) trades that against
+  registers (variant "acc100": budget 100 doubles instead of 66).
+
+Which is better is measured, not guessed:
+
+    python -m asuka_b200.tune_classes build                   # (no GPU) the variant libraries
+    python -m asuka_b200.tune_classes measure w8 w4q --out T  # (GPU) time every class with each library
     cp T asuka_b200/csrc/class_tuning.json && python asuka_b200/csrc/gen_classes.py && python -m asuka_b200.build
 
-A class gets the 4-block bound when it is at least ``MIN_GAIN`` faster with it on every
-workload that contains it; ``gen_classes.py`` reads the table when generating the kernels.
+A class takes a variant when it is at least ``MIN_GAIN`` faster with it on every workload
+that contains the class (the fastest qualifying variant wins); ``gen_classes.py`` reads the
+table when generating the kernels.
 """
 
 from __future__ import annotations
@@ -21,8 +30,17 @@ import subprocess
 import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-VARIANT = os.path.join(HERE, "_tune", "libdfb_minb4.so")
+VARIANTS = {
+    "minb4": dict(defines=["DFB_THREAD_MIN_BLOCKS=4"], gen_env=None,
+                  table=("min_blocks", 4)),
+    "acc100": dict(defines=[], gen_env={"DFB_GEN_NO_TUNING": "1", "DFB_GEN_ACC_BUDGET_DERIV": "100"},
+                   table=("acc_budget", 100)),
+}
 MIN_GAIN = 0.03
+
+
+def _lib(name: str) -> str:
+    return os.path.join(HERE, "_tune", f"libdfb_{name}.so")
 
 
 def _times(workload: str, lib: str | None) -> dict:
@@ -40,18 +58,26 @@ def _times(workload: str, lib: str | None) -> dict:
 
 
 def measure(workloads: list[str]) -> dict:
+    """Time every class with the untuned default build and with each variant; the default build
+    must be generated without a tuning table (``DFB_GEN_NO_TUNING=1``) for a clean baseline."""
     base = {w: _times(w, None) for w in workloads}
-    var = {w: _times(w, VARIANT) for w in workloads}
-    choice, detail = {}, {}
-    keys = sorted({k for w in workloads for k, (_t, kind) in base[w].items() if kind != "warp"})
+    var = {v: {w: _times(w, _lib(v)) for w in workloads} for v in VARIANTS}
+    table = {"min_blocks": {}, "acc_budget": {}}
+    detail = {}
+    keys = sorted({k for w in workloads for k in base[w]})
     for k in keys:
-        gains = [1.0 - var[w][k][0] / base[w][k][0] for w in workloads if k in base[w] and k in var[w]]
-        detail[k] = [round(g, 3) for g in gains]
-        if gains and min(gains) >= MIN_GAIN:
-            choice[k] = 4
+        best = None
+        for v, times in var.items():
+            gains = [1.0 - times[w][k][0] / base[w][k][0] for w in workloads if k in base[w] and k in times[w]]
+            detail.setdefault(k, {})[v] = [round(g, 3) for g in gains]
+            if gains and min(gains) >= MIN_GAIN and (best is None or min(gains) > best[1]):
+                best = (v, min(gains))
+        if best is not None:
+            field, value = VARIANTS[best[0]]["table"]
+            table[field][k] = value
     import torch
 
-    return {"min_blocks": choice, "gain_by_class": detail, "workloads": workloads,
+    return {**table, "gain_by_class": detail, "workloads": workloads,
             "device": torch.cuda.get_device_name(0), "min_gain": MIN_GAIN}
 
 
@@ -61,7 +87,8 @@ def main() -> None:
     if sys.argv[1] == "build":
         from .build import build_variant
 
-        print(build_variant(["DFB_THREAD_MIN_BLOCKS=4"], VARIANT, "minb4"))
+        for v, spec in VARIANTS.items():
+            print(build_variant(spec["defines"], _lib(v), v, gen_env=spec["gen_env"]))
         return
     args = sys.argv[2:]
     out = None

@@ -117,3 +117,26 @@ def test_cart2sph_matches_reference_table():
     T = cart2sph_ao_matrix([0, 1, 2, 3]).numpy()
     assert T.shape == (1 + 3 + 6 + 10, 1 + 3 + 5 + 7)
     assert np.abs(T[4:10, 4:9] - cart2sph_matrix(2)).max() == 0.0
+
+
+def test_class_planner_budget_and_table(tmp_path, monkeypatch):
+    """A larger accumulator budget gives fewer component splits; the generator's tuning-table
+    fields are read per class and can be switched off for variant builds."""
+    import importlib.util
+    import json
+    import os
+
+    src = os.path.join(os.path.dirname(__file__), "..", "asuka_b200", "csrc", "gen_classes.py")
+    spec = importlib.util.spec_from_file_location("gen_classes_t", src)
+    gc = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(gc)
+    gc.HERE = str(tmp_path)
+    fs66, _ = gc.plan(1, 0, 4, True, budget=66)
+    fs100, _ = gc.plan(1, 0, 4, True, budget=100)
+    assert fs100 < fs66
+    (tmp_path / "class_tuning.json").write_text(json.dumps({"min_blocks": {"d104": 4}, "acc_budget": {"d104": 100}}))
+    assert gc.tuning()["d104"] == 4
+    assert gc.plan(1, 0, 4, True) == gc.plan(1, 0, 4, True, budget=100)
+    monkeypatch.setenv("DFB_GEN_NO_TUNING", "1")
+    assert gc.tuning() == {}
+    assert gc.plan(1, 0, 4, True) == gc.plan(1, 0, 4, True, budget=66)
