@@ -21,11 +21,11 @@ int dfb_cls_d0_launch(int la, int lb, int lc, const TmplArgs& g, long nblk, size
         return 1;
     }
     if (lb == 0 && lc == 4) {
-        k_rys_thread<0, 0, 4, 3, true, false, 1><<<dim3((unsigned)nblk, 3), 128, smem, st>>>(g);
+        k_rys_thread<0, 0, 4, 2, true, false, 1><<<dim3((unsigned)nblk, 2), 128, smem, st>>>(g);
         return 1;
     }
     if (lb == 0 && lc == 5) {
-        k_rys_thread<0, 0, 5, 5, true, false, 1><<<dim3((unsigned)nblk, 5), 128, smem, st>>>(g);
+        k_rys_thread<0, 0, 5, 3, true, false, 1><<<dim3((unsigned)nblk, 3), 128, smem, st>>>(g);
         return 1;
     }
     if (lb == 0 && lc == 6) {

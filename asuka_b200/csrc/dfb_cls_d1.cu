@@ -17,19 +17,19 @@ int dfb_cls_d1_launch(int la, int lb, int lc, const TmplArgs& g, long nblk, size
         return 1;
     }
     if (lb == 0 && lc == 3) {
-        k_rys_thread<1, 0, 3, 4, true, false, 1><<<dim3((unsigned)nblk, 4), 128, smem, st>>>(g);
+        k_rys_thread<1, 0, 3, 3, true, false, 1><<<dim3((unsigned)nblk, 3), 128, smem, st>>>(g);
         return 1;
     }
     if (lb == 0 && lc == 4) {
-        k_rys_thread<1, 0, 4, 5, true, false, 1><<<dim3((unsigned)nblk, 5), 128, smem, st>>>(g);
+        k_rys_thread<1, 0, 4, 4, true, false, 1><<<dim3((unsigned)nblk, 4), 128, smem, st>>>(g);
         return 1;
     }
     if (lb == 0 && lc == 5) {
-        k_rys_thread<1, 0, 5, 7, true, false, 1><<<dim3((unsigned)nblk, 7), 128, smem, st>>>(g);
+        k_rys_thread<1, 0, 5, 6, true, false, 1><<<dim3((unsigned)nblk, 6), 128, smem, st>>>(g);
         return 1;
     }
     if (lb == 0 && lc == 6) {
-        k_rys_thread<1, 0, 6, 10, true, false, 1><<<dim3((unsigned)nblk, 10), 128, smem, st>>>(g);
+        k_rys_thread<1, 0, 6, 7, true, false, 1><<<dim3((unsigned)nblk, 7), 128, smem, st>>>(g);
         return 1;
     }
     if (lb == 1 && lc == 0) {
@@ -45,11 +45,11 @@ int dfb_cls_d1_launch(int la, int lb, int lc, const TmplArgs& g, long nblk, size
         return 1;
     }
     if (lb == 1 && lc == 3) {
-        k_rys_thread<1, 1, 3, 10, true, false, 1><<<dim3((unsigned)nblk, 10), 128, smem, st>>>(g);
+        k_rys_thread<1, 1, 3, 5, true, false, 1><<<dim3((unsigned)nblk, 5), 128, smem, st>>>(g);
         return 1;
     }
     if (lb == 1 && lc == 4) {
-        k_rys_thread<1, 1, 4, 15, true, false, 1><<<dim3((unsigned)nblk, 15), 128, smem, st>>>(g);
+        k_rys_thread<1, 1, 4, 8, true, false, 1><<<dim3((unsigned)nblk, 8), 128, smem, st>>>(g);
         return 1;
     }
     if (lb == 1 && lc == 5) {

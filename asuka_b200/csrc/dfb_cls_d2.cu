@@ -9,19 +9,19 @@ int dfb_cls_d2_launch(int la, int lb, int lc, const TmplArgs& g, long nblk, size
         return 1;
     }
     if (lb == 0 && lc == 1) {
-        k_rys_thread<2, 0, 1, 3, true, false, 4><<<dim3((unsigned)nblk, 3), 128, smem, st>>>(g);
+        k_rys_thread<2, 0, 1, 2, true, false, 1><<<dim3((unsigned)nblk, 2), 128, smem, st>>>(g);
         return 1;
     }
     if (lb == 0 && lc == 2) {
-        k_rys_thread<2, 0, 2, 6, true, false, 4><<<dim3((unsigned)nblk, 6), 128, smem, st>>>(g);
+        k_rys_thread<2, 0, 2, 3, true, false, 1><<<dim3((unsigned)nblk, 3), 128, smem, st>>>(g);
         return 1;
     }
     if (lb == 0 && lc == 3) {
-        k_rys_thread<2, 0, 3, 10, true, false, 4><<<dim3((unsigned)nblk, 10), 128, smem, st>>>(g);
+        k_rys_thread<2, 0, 3, 5, true, false, 1><<<dim3((unsigned)nblk, 5), 128, smem, st>>>(g);
         return 1;
     }
     if (lb == 0 && lc == 4) {
-        k_rys_thread<2, 0, 4, 15, true, false, 4><<<dim3((unsigned)nblk, 15), 128, smem, st>>>(g);
+        k_rys_thread<2, 0, 4, 8, true, false, 1><<<dim3((unsigned)nblk, 8), 128, smem, st>>>(g);
         return 1;
     }
     if (lb == 0 && lc == 5) {
@@ -37,27 +37,27 @@ int dfb_cls_d2_launch(int la, int lb, int lc, const TmplArgs& g, long nblk, size
         return 1;
     }
     if (lb == 1 && lc == 1) {
-        k_rys_thread<2, 1, 1, 2, true, true, 1><<<dim3((unsigned)nblk, 4), 128, smem, st>>>(g);
+        k_rys_thread<2, 1, 1, 3, true, false, 1><<<dim3((unsigned)nblk, 3), 128, smem, st>>>(g);
         return 1;
     }
     if (lb == 1 && lc == 2) {
-        k_rys_thread<2, 1, 2, 3, true, true, 1><<<dim3((unsigned)nblk, 6), 128, smem, st>>>(g);
+        k_rys_thread<2, 1, 2, 6, true, false, 1><<<dim3((unsigned)nblk, 6), 128, smem, st>>>(g);
         return 1;
     }
     if (lb == 1 && lc == 3) {
-        k_rys_thread<2, 1, 3, 5, true, true, 1><<<dim3((unsigned)nblk, 10), 128, smem, st>>>(g);
+        k_rys_thread<2, 1, 3, 10, true, false, 1><<<dim3((unsigned)nblk, 10), 128, smem, st>>>(g);
         return 1;
     }
     if (lb == 1 && lc == 4) {
-        k_rys_thread<2, 1, 4, 8, true, true, 1><<<dim3((unsigned)nblk, 16), 128, smem, st>>>(g);
+        k_rys_thread<2, 1, 4, 15, true, false, 1><<<dim3((unsigned)nblk, 15), 128, smem, st>>>(g);
         return 1;
     }
     if (lb == 1 && lc == 5) {
-        k_rys_thread<2, 1, 5, 21, true, true, 4><<<dim3((unsigned)nblk, 42), 128, smem, st>>>(g);
+        k_rys_thread<2, 1, 5, 21, true, false, 1><<<dim3((unsigned)nblk, 21), 128, smem, st>>>(g);
         return 1;
     }
     if (lb == 1 && lc == 6) {
-        k_rys_thread<2, 1, 6, 28, true, true, 1><<<dim3((unsigned)nblk, 56), 128, smem, st>>>(g);
+        k_rys_thread<2, 1, 6, 28, true, false, 1><<<dim3((unsigned)nblk, 28), 128, smem, st>>>(g);
         return 1;
     }
     if (lb == 2 && lc == 0) {

@@ -9,7 +9,7 @@ int dfb_cls_d3_launch(int la, int lb, int lc, const TmplArgs& g, long nblk, size
         return 1;
     }
     if (lb == 0 && lc == 1) {
-        k_rys_thread<3, 0, 1, 2, true, true, 1><<<dim3((unsigned)nblk, 4), 128, smem, st>>>(g);
+        k_rys_thread<3, 0, 1, 3, true, false, 1><<<dim3((unsigned)nblk, 3), 128, smem, st>>>(g);
         return 1;
     }
     if (lb == 0 && lc == 2) {
@@ -17,7 +17,7 @@ int dfb_cls_d3_launch(int la, int lb, int lc, const TmplArgs& g, long nblk, size
         return 1;
     }
     if (lb == 0 && lc == 3) {
-        k_rys_thread<3, 0, 3, 5, true, true, 1><<<dim3((unsigned)nblk, 10), 128, smem, st>>>(g);
+        k_rys_thread<3, 0, 3, 10, true, false, 1><<<dim3((unsigned)nblk, 10), 128, smem, st>>>(g);
         return 1;
     }
     if (lb == 0 && lc == 4) {

@@ -41,11 +41,11 @@ int dfb_cls_i2_launch(int la, int lb, int lc, const TmplArgs& g, long nblk, size
         return 1;
     }
     if (lb == 1 && lc == 2) {
-        k_rys_thread<2, 1, 2, 3, false, false, 1><<<dim3((unsigned)nblk, 3), 128, smem, st>>>(g);
+        k_rys_thread<2, 1, 2, 2, false, false, 1><<<dim3((unsigned)nblk, 2), 128, smem, st>>>(g);
         return 1;
     }
     if (lb == 1 && lc == 3) {
-        k_rys_thread<2, 1, 3, 5, false, false, 1><<<dim3((unsigned)nblk, 5), 128, smem, st>>>(g);
+        k_rys_thread<2, 1, 3, 3, false, false, 1><<<dim3((unsigned)nblk, 3), 128, smem, st>>>(g);
         return 1;
     }
     if (lb == 1 && lc == 4) {
@@ -53,7 +53,7 @@ int dfb_cls_i2_launch(int la, int lb, int lc, const TmplArgs& g, long nblk, size
         return 1;
     }
     if (lb == 1 && lc == 5) {
-        k_rys_thread<2, 1, 5, 21, false, false, 1><<<dim3((unsigned)nblk, 21), 128, smem, st>>>(g);
+        k_rys_thread<2, 1, 5, 7, false, false, 1><<<dim3((unsigned)nblk, 7), 128, smem, st>>>(g);
         return 1;
     }
     if (lb == 1 && lc == 6) {

@@ -41,15 +41,15 @@ int dfb_cls_i3_launch(int la, int lb, int lc, const TmplArgs& g, long nblk, size
         return 1;
     }
     if (lb == 1 && lc == 2) {
-        k_rys_thread<3, 1, 2, 6, false, false, 1><<<dim3((unsigned)nblk, 6), 128, smem, st>>>(g);
+        k_rys_thread<3, 1, 2, 3, false, false, 1><<<dim3((unsigned)nblk, 3), 128, smem, st>>>(g);
         return 1;
     }
     if (lb == 1 && lc == 3) {
-        k_rys_thread<3, 1, 3, 10, false, false, 1><<<dim3((unsigned)nblk, 10), 128, smem, st>>>(g);
+        k_rys_thread<3, 1, 3, 5, false, false, 1><<<dim3((unsigned)nblk, 5), 128, smem, st>>>(g);
         return 1;
     }
     if (lb == 1 && lc == 4) {
-        k_rys_thread<3, 1, 4, 15, false, false, 1><<<dim3((unsigned)nblk, 15), 128, smem, st>>>(g);
+        k_rys_thread<3, 1, 4, 8, false, false, 1><<<dim3((unsigned)nblk, 8), 128, smem, st>>>(g);
         return 1;
     }
     if (lb == 1 && lc == 5) {
@@ -58,6 +58,26 @@ int dfb_cls_i3_launch(int la, int lb, int lc, const TmplArgs& g, long nblk, size
     }
     if (lb == 1 && lc == 6) {
         k_rys_thread<3, 1, 6, 28, false, false, 1><<<dim3((unsigned)nblk, 28), 128, smem, st>>>(g);
+        return 1;
+    }
+    if (lb == 2 && lc == 0) {
+        k_rys_thread<3, 2, 0, 1, false, false, 1><<<dim3((unsigned)nblk, 1), 128, smem, st>>>(g);
+        return 1;
+    }
+    if (lb == 2 && lc == 1) {
+        k_rys_thread<3, 2, 1, 3, false, false, 1><<<dim3((unsigned)nblk, 3), 128, smem, st>>>(g);
+        return 1;
+    }
+    if (lb == 2 && lc == 2) {
+        k_rys_thread<3, 2, 2, 6, false, false, 1><<<dim3((unsigned)nblk, 6), 128, smem, st>>>(g);
+        return 1;
+    }
+    if (lb == 2 && lc == 3) {
+        k_rys_thread<3, 2, 3, 10, false, false, 1><<<dim3((unsigned)nblk, 10), 128, smem, st>>>(g);
+        return 1;
+    }
+    if (lb == 2 && lc == 5) {
+        k_rys_thread<3, 2, 5, 21, false, false, 1><<<dim3((unsigned)nblk, 21), 128, smem, st>>>(g);
         return 1;
     }
     return 0;

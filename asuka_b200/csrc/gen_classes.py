@@ -69,13 +69,13 @@ def plan(la, lb, lc, deriv, budget=None):
     ``budget`` overrides the accumulator budget; without it the measured per-class table
     (``class_tuning.json``, "acc_budget") or the default ACC_BUDGET applies.  The
     environment variable DFB_GEN_ACC_BUDGET_DERIV sets the derivative default (the tuner's
-    variant builds).
+    variant builds) and DFB_GEN_ACC_BUDGET_INT the integral one.
     """
     if budget is None:
         budget = tuning("acc_budget").get(_key(la, lb, lc, deriv))
     if budget is None:
-        env = os.environ.get("DFB_GEN_ACC_BUDGET_DERIV")
-        budget = int(env) if (env and deriv) else ACC_BUDGET[deriv]
+        env = os.environ.get("DFB_GEN_ACC_BUDGET_DERIV" if deriv else "DFB_GEN_ACC_BUDGET_INT")
+        budget = int(env) if env else ACC_BUDGET[deriv]
     nm = la + lb + (1 if deriv else 0)
     nf = ncart(lc)
     modes = [(1, False), (None, True)] if deriv else [(0, False)]

@@ -6,10 +6,12 @@ Two knobs are tuned per angular class, each against the default build:
   registers (the classes use 150-170, i.e. 3 resident blocks per SM); capping them at 128
   (4 blocks per SM) helps the classes whose working set still fits and hurts those that spill
   (variant "minb4");
-* the aux-component split: a derivative class is split over FS threads per task so that one
-  thread's accumulators fit a register budget; every extra split repeats the task's Rys roots
-  and recurrence tables, a larger budget (fewer, heavier threads) trades that against
-  registers (variant "acc100": budget 100 doubles instead of 66).
+* the aux-component split: a class is split over FS threads per task so that one thread's
+  accumulators fit a register budget; every extra split repeats the task's Rys roots and
+  recurrence tables, a larger budget (fewer, heavier threads) trades that against registers
+  (variants "acc100" and "acc136": derivative budgets 100 and 136 doubles instead of 66,
+  integral budgets 64 and 96 instead of 40); a larger budget also moves classes from the
+  generic warp path onto the thread kernels.
 
 Which is better is measured, not guessed:
 
@@ -33,9 +35,15 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 VARIANTS = {
     "minb4": dict(defines=["DFB_THREAD_MIN_BLOCKS=4"], gen_env=None,
                   table=("min_blocks", 4)),
-    "acc100": dict(defines=[], gen_env={"DFB_GEN_NO_TUNING": "1", "DFB_GEN_ACC_BUDGET_DERIV": "100"},
-                   table=("acc_budget", 100)),
+    "acc100": dict(defines=[], gen_env={"DFB_GEN_NO_TUNING": "1", "DFB_GEN_ACC_BUDGET_DERIV": "100",
+                                        "DFB_GEN_ACC_BUDGET_INT": "64"},
+                   table=("acc_budget", None)),
+    "acc136": dict(defines=[], gen_env={"DFB_GEN_NO_TUNING": "1", "DFB_GEN_ACC_BUDGET_DERIV": "136",
+                                        "DFB_GEN_ACC_BUDGET_INT": "96"},
+                   table=("acc_budget", None)),
 }
+# accumulator budgets of the generated variants (derivative, integral classes)
+_BUDGETS = {"acc100": (100, 64), "acc136": (136, 96)}
 MIN_GAIN = 0.03
 
 
@@ -74,6 +82,8 @@ def measure(workloads: list[str]) -> dict:
                 best = (v, min(gains))
         if best is not None:
             field, value = VARIANTS[best[0]]["table"]
+            if value is None:  # generated variant: the class's budget in that variant
+                value = _BUDGETS[best[0]][0 if k.startswith("d") else 1]
             table[field][k] = value
     import torch
 
