@@ -55,8 +55,8 @@ def _workload():
 
 # DRAM bytes (read + write) of one 3c derivative contraction of this workload (all class launches of
 # one gradient), from one ncu capture: --metrics dram__bytes_read.sum,dram__bytes_write.sum -k regex:k_rys
-# on `python -m asuka_b200.profile_step --workload w8 --only deriv3c --steps 1` (3.639e9 + 0.039e9).
-DERIV3C_DRAM_BYTES = 3.679e9
+# on `python -m asuka_b200.profile_step --workload w8 --only deriv3c --steps 1` (3.467e9 + 0.025e9).
+DERIV3C_DRAM_BYTES = 3.492e9
 
 
 def flops_3c(ao, aux, deriv: bool = False) -> float:
