@@ -22,6 +22,10 @@ class PairSide(ctypes.Structure):
         ("b_dummy", ctypes.c_int)]
 
 
+class TcOperand(ctypes.Structure):
+    _fields_ = [("ptr", ctypes.c_void_p)] + [(n, ctypes.c_long) for n in ("s_row", "s_kq", "s_k1", "nk1", "s_batch")]
+
+
 class AuxSide(ctypes.Structure):
     _fields_ = [(n, ctypes.c_void_p) for n in ("cxyz", "pstart", "nprim", "pexp", "pcoef", "aostart", "atom")]
 
@@ -40,6 +44,21 @@ _SIGS = {
                                                           ctypes.c_long, ctypes.c_long, ctypes.c_int, _d,
                                                           ctypes.c_long, ctypes.c_long, ctypes.c_long, _d,
                                                           ctypes.c_int, _d, ctypes.c_long, _d]),
+    "dfb_rys_int_prec": (ctypes.c_int, [ctypes.c_int] * 3 + [ctypes.POINTER(PairSide), ctypes.POINTER(AuxSide), _d,
+                                                             _d, ctypes.c_long, ctypes.c_long, ctypes.c_int,
+                                                             ctypes.c_int, _d, ctypes.c_long, ctypes.c_long,
+                                                             ctypes.c_long, _d, ctypes.c_long, _d]),
+    "dfb_rys_deriv_prec": (ctypes.c_int, [ctypes.c_int] * 3 + [ctypes.POINTER(PairSide), ctypes.POINTER(AuxSide), _d,
+                                                               _d, ctypes.c_long, ctypes.c_long, ctypes.c_int,
+                                                               ctypes.c_int, _d, ctypes.c_long, ctypes.c_long,
+                                                               ctypes.c_long, _d, ctypes.c_int, _d, ctypes.c_long,
+                                                               _d]),
+    "dfb_tc_gemm": (ctypes.c_int, [ctypes.c_long] * 4 + [ctypes.POINTER(TcOperand), ctypes.POINTER(TcOperand), _d,
+                                                          ctypes.c_long, ctypes.c_long, ctypes.c_int, ctypes.c_int,
+                                                          ctypes.c_int, ctypes.c_long, _d]),
+    "dfb_tc_error": (ctypes.c_int, [ctypes.c_int]),
+    "dfb_fp32_fma_probe": (ctypes.c_int, [_d, ctypes.c_int, ctypes.c_int, ctypes.c_int, _d]),
+    "dfb_launch_count": (ctypes.c_long, []),
     "dfb_rys_scratch_doubles": (ctypes.c_long, [ctypes.c_int] * 3 + [ctypes.c_long, ctypes.c_int]),
     "dfb_fp64_fma_probe": (ctypes.c_int, [_d, ctypes.c_int, ctypes.c_int, ctypes.c_int, _d]),
     "dfb_rys_int_noalloc": (ctypes.c_int, [ctypes.c_int] * 3 + [ctypes.POINTER(PairSide), ctypes.POINTER(AuxSide), _d,
@@ -64,7 +83,9 @@ def lib() -> ctypes.CDLL:
                 "(the DF engine has no CPU fallback)")
         L = ctypes.CDLL(LIB_PATH)
         for name, (res, args) in _SIGS.items():
-            fn = getattr(L, name)
+            fn = getattr(L, name, None)
+            if fn is None:  # a library built before this entry point existed: fails where it is called
+                continue
             fn.restype = res
             fn.argtypes = args
         _LIB = L

@@ -40,6 +40,7 @@ from . import basis as bm
 from . import geometry as geo
 from . import linalg as _la
 from . import mixed as _mixed
+from . import tc as _tc
 from .df import DFEngine, ScratchHolder, cholesky_metric
 
 
@@ -142,12 +143,11 @@ class BatchedDFJK:
         K = m.K
         K.zero_()
         qb = max(1, (1 << 27) // max(nao * nocc, 1))
-        for q0 in range(0, naux, qb):
+        if mixed:
+            _tc.syrk_qblocks(W3, out=K)  # split-BF16 tcgen05 update, W read in place
+        for q0 in range(0, 0 if mixed else naux, qb):
             Wc = W3[q0:q0 + qb].permute(1, 0, 2).reshape(nao, -1)
-            if mixed and nao >= _mixed.MIN_DIM:
-                K += _mixed.syrk(Wc)
-            else:
-                K.addmm_(Wc, Wc.T)
+            K.addmm_(Wc, Wc.T)
         K.copy_(0.5 * (K + K.T))
         J = m.J
         J.zero_()

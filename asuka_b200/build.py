@@ -9,6 +9,7 @@ import glob
 import os
 import subprocess
 import sys
+import time
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
@@ -22,12 +23,44 @@ def sources() -> list[str]:
 
 
 def needs_build() -> bool:
+    """True when the library is missing or older than a source, a header a source includes, or
+    when a source has no object yet."""
     if not os.path.exists(OUT):
         return True
     t = os.path.getmtime(OUT)
-    deps = sources() + glob.glob(os.path.join(CSRC, "*.cuh")) + glob.glob(os.path.join(CSRC, "*.h"))
-    deps.append(os.path.join(HERE, "..", "include", "dfb.h"))
-    return any(os.path.getmtime(p) > t for p in deps if os.path.exists(p))
+    objdir = os.path.join(HERE, "_build")
+    for src in sources():
+        obj = os.path.join(objdir, os.path.basename(src)[:-3] + ".o")
+        if not os.path.exists(obj) or os.path.getmtime(obj) > t:
+            return True
+        if any(os.path.getmtime(p) > t for p in [src, *_local_includes(src)]):
+            return True
+    return False
+
+
+def _local_includes(path: str, seen: set | None = None) -> set:
+    """Headers of this source tree that ``path`` includes, directly or through other headers
+    (#include "..." lines), so that a header change rebuilds only the objects that use it."""
+    import re
+
+    seen = set() if seen is None else seen
+    try:
+        with open(path) as f:
+            txt = f.read()
+    except OSError:
+        return seen
+    for name in re.findall(r'^\s*#\s*include\s+"([^"]+)"', txt, flags=re.M):
+        h = os.path.normpath(os.path.join(os.path.dirname(path), name))
+        if h not in seen and os.path.exists(h):
+            seen.add(h)
+            _local_includes(h, seen)
+    return seen
+
+
+def _wait_slot(procs: list, jobs: int) -> None:
+    """Block until fewer than ``jobs`` of the compiler processes are still running."""
+    while sum(1 for p in procs if p.poll() is None) >= jobs:
+        time.sleep(0.2)
 
 
 def _flags_changed(objdir: str, flags: list[str]) -> bool:
@@ -49,20 +82,17 @@ def build(force: bool = False, verbose: bool = False, jobs: int | None = None) -
     procs = []
     objs = []
     jobs = jobs or max(1, os.cpu_count() or 1)
-    headers = glob.glob(os.path.join(CSRC, "*.cuh")) + glob.glob(os.path.join(CSRC, "*.h"))
-    headers.append(os.path.join(HERE, "..", "include", "dfb.h"))
-    t_hdr = max(os.path.getmtime(h) for h in headers if os.path.exists(h))
     for src in sources():
         obj = os.path.join(objdir, os.path.basename(src)[:-3] + ".o")
         objs.append(obj)
-        if (not force and os.path.exists(obj) and os.path.getmtime(obj) >= os.path.getmtime(src)
-                and os.path.getmtime(obj) >= t_hdr and not _flags_changed(objdir, compile_flags)):
+        t_dep = max([os.path.getmtime(src)] + [os.path.getmtime(h) for h in _local_includes(src)])
+        if (not force and os.path.exists(obj) and os.path.getmtime(obj) >= t_dep
+                and not _flags_changed(objdir, compile_flags)):
             continue
         cmd = [nvcc, *compile_flags, "-c", src, "-o", obj]
         if verbose:
             print(" ".join(cmd), flush=True)
-        while len([p for p in procs if p.poll() is None]) >= jobs:
-            procs[0].wait() if procs[0].poll() is None else procs.pop(0)
+        _wait_slot(procs, jobs)
         procs.append(subprocess.Popen(cmd, cwd=CSRC))
     for p in procs:
         if p.wait() != 0:
@@ -111,8 +141,7 @@ def build_variant(defines: list[str], out: str, tag: str, jobs: int | None = Non
             continue
         obj = os.path.join(vdir, base + ".o")
         objs.append(obj)
-        while len([p for p in procs if p.poll() is None]) >= jobs:
-            procs[0].wait() if procs[0].poll() is None else procs.pop(0)
+        _wait_slot(procs, jobs)
         procs.append(subprocess.Popen([nvcc, *compile_flags, *inc, "-c", src, "-o", obj], cwd=srcdir))
     for p in procs:
         if p.wait() != 0:

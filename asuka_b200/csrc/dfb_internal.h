@@ -6,4 +6,6 @@ namespace dfb {
 void clear_error();
 int set_error(int code, const char* fmt, ...);
 int set_cuda_error(const char* what, cudaError_t e);
+// count kernel launches made by the library (dfb_launch_count)
+void count_launches(long n);
 }  // namespace dfb

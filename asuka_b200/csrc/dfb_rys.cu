@@ -614,6 +614,7 @@ static int launch_rys(const ClassInfo& ci, const dfb_pair_side_t* ps, const dfb_
                                                                           naux_grid, mode, out, sP, sM, sN, bar, sbP,
                                                                           sbM, sbN, grad, natm, smem_grad, scratch,
                                                                           slot);
+        count_launches(2);
         e = cudaGetLastError();
         if (e != cudaSuccess) return set_cuda_error("k_rys launch", e);
     }
@@ -625,7 +626,7 @@ static int dispatch_rys(int la, int lb, int lc, const dfb_pair_side_t* ps, const
                         const int* task_pair, const int* task_aux, long ntask, long naux_grid, int mode, double* out,
                         long sP, long sM, long sN, const double* bar, long sbP, long sbM, long sbN, double* grad, int natm,
                         double* scratch, long scratch_doubles, cudaStream_t st, int query_only, long* need,
-                        int fit_grid_to_scratch = 0) {
+                        int fit_grid_to_scratch = 0, int f32 = 0) {
     if (la < 0 || lb < 0 || lc < 0 || la > DFB_LMAX || lb > DFB_LMAX || lc > DFB_LMAX)
         return set_error(DFB_ERR_UNSUPPORTED, "angular momentum out of range (la=%d lb=%d lc=%d, max %d)", la, lb, lc,
                          DFB_LMAX);
@@ -678,13 +679,16 @@ static int dispatch_rys(int la, int lb, int lc, const dfb_pair_side_t* ps, const
         const size_t smem = (g.smem_grad ? sizeof(double) * natm * 3 : 0) + sizeof(double) * 128 * 2 * ci.nr;
         const long nblk = (ntask + 127) / 128;
         if (nblk > 2147483647L) return set_error(DFB_ERR_INVALID, "too many tasks in one class launch");
-        if (tmpl_launch(la, lb, lc, DERIV, g, nblk, smem, st)) {
+        if (tmpl_launch(la, lb, lc, DERIV, f32 != 0, g, nblk, smem, st)) {
+            count_launches(1);
             cudaError_t e = cudaGetLastError();
             if (e != cudaSuccess) return set_cuda_error("k_rys_thread launch", e);
             return DFB_OK;
         }
     }
-    if (query_only && getenv("DFB_DISABLE_TMPL") == nullptr && tmpl_has(la, lb, lc, DERIV)) {
+    // scratch is needed only when one of the two component types runs this class on the generic kernel
+    if (query_only && getenv("DFB_DISABLE_TMPL") == nullptr && tmpl_has(la, lb, lc, DERIV, false) &&
+        tmpl_has(la, lb, lc, DERIV, true)) {
         *need = 0;
         return DFB_OK;
     }
@@ -752,19 +756,46 @@ extern "C" int dfb_pair_tables(const double* cxyz, const int* shell_pstart, cons
     k_pair_tables<<<blocks, 256, 0, (cudaStream_t)stream>>>(cxyz, shell_pstart, shell_nprim, pexp, pcoef, sp_A, sp_B,
                                                             sp_pstart, pp_sp, pp_local, npp, b_dummy, eta, Px, Py,
                                                             Pz, cK, ea, eb);
+    count_launches(1);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return set_cuda_error("k_pair_tables launch", e);
     return DFB_OK;
 }
 
-extern "C" int dfb_rys_int(int la, int lb, int lc, const dfb_pair_side_t* ps, const dfb_aux_side_t* aux,
-                           const int* task_pair, const int* task_aux, long ntask, long naux_grid, int mode, double* out, long sP,
-                           long sM, long sN, double* scratch, long scratch_doubles, void* stream) {
+extern "C" int dfb_rys_int_prec(int la, int lb, int lc, const dfb_pair_side_t* ps, const dfb_aux_side_t* aux,
+                                const int* task_pair, const int* task_aux, long ntask, long naux_grid, int mode,
+                                int precision, double* out, long sP, long sM, long sN, double* scratch,
+                                long scratch_doubles, void* stream) {
     clear_error();
     if (!ps || !aux || (ntask > 0 && (!task_pair || !task_aux || !out)) || (mode != 0 && mode != 1))
         return set_error(DFB_ERR_INVALID, "invalid arguments to dfb_rys_int");
+    if (precision != DFB_PREC_FP64 && precision != DFB_PREC_MIXED)
+        return set_error(DFB_ERR_INVALID, "unknown precision %d", precision);
     return dispatch_rys<false>(la, lb, lc, ps, aux, task_pair, task_aux, ntask, naux_grid, mode, out, sP, sM, sN, nullptr, 0, 0,
-                               0, nullptr, 0, scratch, scratch_doubles, (cudaStream_t)stream, 0, nullptr);
+                               0, nullptr, 0, scratch, scratch_doubles, (cudaStream_t)stream, 0, nullptr, 0,
+                               precision == DFB_PREC_MIXED);
+}
+
+extern "C" int dfb_rys_int(int la, int lb, int lc, const dfb_pair_side_t* ps, const dfb_aux_side_t* aux,
+                           const int* task_pair, const int* task_aux, long ntask, long naux_grid, int mode, double* out, long sP,
+                           long sM, long sN, double* scratch, long scratch_doubles, void* stream) {
+    return dfb_rys_int_prec(la, lb, lc, ps, aux, task_pair, task_aux, ntask, naux_grid, mode, DFB_PREC_FP64, out, sP,
+                            sM, sN, scratch, scratch_doubles, stream);
+}
+
+extern "C" int dfb_rys_deriv_prec(int la, int lb, int lc, const dfb_pair_side_t* ps, const dfb_aux_side_t* aux,
+                                  const int* task_pair, const int* task_aux, long ntask, long naux_grid, int mode,
+                                  int precision, const double* bar, long sbP, long sbM, long sbN, double* grad,
+                                  int natm, double* scratch, long scratch_doubles, void* stream) {
+    clear_error();
+    if (!ps || !aux || (ntask > 0 && (!task_pair || !task_aux || !bar || !grad)) || (mode != 0 && mode != 1) ||
+        natm < 1)
+        return set_error(DFB_ERR_INVALID, "invalid arguments to dfb_rys_deriv");
+    if (precision != DFB_PREC_FP64 && precision != DFB_PREC_MIXED)
+        return set_error(DFB_ERR_INVALID, "unknown precision %d", precision);
+    return dispatch_rys<true>(la, lb, lc, ps, aux, task_pair, task_aux, ntask, naux_grid, mode, nullptr, 0, 0, 0, bar, sbP, sbM,
+                              sbN, grad, natm, scratch, scratch_doubles, (cudaStream_t)stream, 0, nullptr, 0,
+                              precision == DFB_PREC_MIXED);
 }
 
 extern "C" int dfb_rys_deriv(int la, int lb, int lc, const dfb_pair_side_t* ps, const dfb_aux_side_t* aux,
@@ -772,12 +803,8 @@ extern "C" int dfb_rys_deriv(int la, int lb, int lc, const dfb_pair_side_t* ps, 
                              const double* bar,
                              long sbP, long sbM, long sbN, double* grad, int natm, double* scratch,
                              long scratch_doubles, void* stream) {
-    clear_error();
-    if (!ps || !aux || (ntask > 0 && (!task_pair || !task_aux || !bar || !grad)) || (mode != 0 && mode != 1) ||
-        natm < 1)
-        return set_error(DFB_ERR_INVALID, "invalid arguments to dfb_rys_deriv");
-    return dispatch_rys<true>(la, lb, lc, ps, aux, task_pair, task_aux, ntask, naux_grid, mode, nullptr, 0, 0, 0, bar, sbP, sbM,
-                              sbN, grad, natm, scratch, scratch_doubles, (cudaStream_t)stream, 0, nullptr);
+    return dfb_rys_deriv_prec(la, lb, lc, ps, aux, task_pair, task_aux, ntask, naux_grid, mode, DFB_PREC_FP64, bar,
+                              sbP, sbM, sbN, grad, natm, scratch, scratch_doubles, stream);
 }
 
 extern "C" long dfb_rys_scratch_doubles(int la, int lb, int lc, long ntask, int deriv) {
@@ -816,9 +843,13 @@ extern "C" long dfb_rys_scratch_doubles(int la, int lb, int lc, long ntask, int 
 // calls share the array: each task overwrites the part it reads, so nothing
 // needs clearing between calls, but calls that overlap on the GPU (different
 // streams, or concurrent host threads) race on it and must be serialised by
-// the caller.  When a class needs more than the array holds per block of the
-// persistent grid, the grid is shrunk to fit; when not even one block fits, the
-// call fails with DFB_ERR_UNSUPPORTED and a message naming the sizes.
+// the caller.  The generic path needs one slot per task (the contracted
+// intermediate: ne * nf doubles), so the class's tasks run in batches of
+// floor(DFB_NOALLOC_SCRATCH_DOUBLES / slot) tasks, one accumulation and one
+// epilogue launch per batch, in order on the caller's stream.  A class fails
+// with DFB_ERR_UNSUPPORTED only when a single task's slot exceeds the array,
+// which no class with l <= 8 on every centre does (the largest slot is about
+// 38,000 doubles).
 // ---------------------------------------------------------------------------
 
 #define DFB_NOALLOC_SCRATCH_DOUBLES (1L << 20)

@@ -23,7 +23,7 @@
 #pragma once
 #include <utility>
 
-#include "../../include/dfb.h"
+#include "../../include/dfb_types.h"
 #include "dfb_common.cuh"
 
 #define DFB_RYS_DEG 9  // polynomial degree of the Rys table (checked at upload)
@@ -165,28 +165,29 @@ __device__ __forceinline__ void rys_eval_smem(const RysTable& tab, double T, dou
     }
 }
 
-template <int NM, int MM>
-__device__ __forceinline__ void build_G_t(double (&G)[NM + 1][MM + 1], double g00, double C, double Cp, double B0,
-                                          double B1, double B1p) {
+// 2D recurrence tables of one root and direction in the component type R (double, or
+// float for the mixed-precision kernels; the coefficients arrive already rounded to R).
+template <int NM, int MM, typename R>
+__device__ __forceinline__ void build_G_t(R (&G)[NM + 1][MM + 1], R g00, R C, R Cp, R B0, R B1, R B1p) {
     G[0][0] = g00;
 #pragma unroll
     for (int a = 1; a <= NM; ++a) {
-        double v = C * G[a - 1][0];
-        if (a >= 2) v += B1 * (double)(a - 1) * G[a >= 2 ? a - 2 : 0][0];
+        R v = C * G[a - 1][0];
+        if (a >= 2) v += B1 * (R)(a - 1) * G[a >= 2 ? a - 2 : 0][0];
         G[a][0] = v;
     }
 #pragma unroll
     for (int b = 1; b <= MM; ++b) {
-        double v = Cp * G[0][b - 1];
-        if (b >= 2) v += B1p * (double)(b - 1) * G[0][b >= 2 ? b - 2 : 0];
+        R v = Cp * G[0][b - 1];
+        if (b >= 2) v += B1p * (R)(b - 1) * G[0][b >= 2 ? b - 2 : 0];
         G[0][b] = v;
     }
 #pragma unroll
     for (int a = 1; a <= NM; ++a) {
 #pragma unroll
         for (int b = 1; b <= MM; ++b) {
-            double v = (double)a * B0 * G[a - 1][b - 1] + Cp * G[a][b - 1];
-            if (b >= 2) v += B1p * (double)(b - 1) * G[a][b >= 2 ? b - 2 : 0];
+            R v = (R)a * B0 * G[a - 1][b - 1] + Cp * G[a][b - 1];
+            if (b >= 2) v += B1p * (R)(b - 1) * G[a][b >= 2 ? b - 2 : 0];
             G[a][b] = v;
         }
     }
@@ -219,8 +220,12 @@ static constexpr double kTwoPi52_t = 2.0 * 3.14159265358979323846264338327950288
 //   MODE 2: derivative, centre A U  over [LA-1, LA+LB-1], WA over [LA+1, LA+LB+1]
 //   MODE 3: derivative, centre B U  over [LA, LA+LB-1],   WB over [LA, LA+LB+1]
 // Centre C gets -(A + B) from the pass(es) that computed them.
-template <int LA_, int LB_, int LC_, int FS_, int FSI_, int MODE_>
+// R: type of the recurrence tables and the accumulators (double; float in the
+// mixed-precision kernels, where roots, weights, prefactors, the horizontal
+// recurrence, the adjoint contraction and the gradient stay FP64).
+template <int LA_, int LB_, int LC_, int FS_, int FSI_, int MODE_, typename R_ = double>
 struct Cls {
+    using R = R_;
     static constexpr int LA = LA_, LB = LB_, LC = LC_, FS = FS_, FSI = FSI_, MODE = MODE_;
     static constexpr bool DERIV = MODE > 0;
     static constexpr int NR = (LA + LB + LC + (DERIV ? 1 : 0)) / 2 + 1;
@@ -258,36 +263,35 @@ struct Cls {
     }
     static constexpr int MDX = md(0), MDY = md(1), MDZ = md(2);
     struct Acc {
-        double a0[NE0][NL];
-        double a1[NE1][NL];
-        double a2[NE2][NL];
+        R a0[NE0][NL];
+        R a1[NE1][NL];
+        R a2[NE2][NL];
     };
-    typedef double GtX[NM + 1][MDX + 1];
-    typedef double GtY[NM + 1][MDY + 1];
-    typedef double GtZ[NM + 1][MDZ + 1];
+    typedef R GtX[NM + 1][MDX + 1];
+    typedef R GtY[NM + 1][MDY + 1];
+    typedef R GtZ[NM + 1][MDZ + 1];
     typedef double ABt[3][LB + 2];
 
     template <int K>
-    __device__ __forceinline__ static double& at(Acc& A, int e, int f) {
+    __device__ __forceinline__ static R& at(Acc& A, int e, int f) {
         if constexpr (K == 0) return A.a0[e][f];
         else if constexpr (K == 1) return A.a1[e][f];
         else return A.a2[e][f];
     }
     template <int K>
     __device__ __forceinline__ static double get(const Acc& A, int e, int f) {
-        if constexpr (K == 0) return A.a0[e][f];
-        else if constexpr (K == 1) return A.a1[e][f];
-        else return A.a2[e][f];
+        if constexpr (K == 0) return (double)A.a0[e][f];
+        else if constexpr (K == 1) return (double)A.a1[e][f];
+        else return (double)A.a2[e][f];
     }
 
     // accumulate element J = e*NL + f of array K for one root
     template <int K, int J>
-    __device__ __forceinline__ static void acc_one(Acc& A, const GtX& Gx, const GtY& Gy, const GtZ& Gz, double a2,
-                                                   double b2) {
+    __device__ __forceinline__ static void acc_one(Acc& A, const GtX& Gx, const GtY& Gy, const GtZ& Gz, R a2, R b2) {
         constexpr int e = J / NL, f = J % NL;
         constexpr int ex = c_ex(lo(K), e), ey = c_ey(lo(K), e), ez = c_ez(lo(K), e);
         constexpr int fx = c_cx(LC, F0 + f), fy = c_cy(LC, F0 + f), fz = c_cz(LC, F0 + f);
-        const double t = Gx[ex][fx] * Gy[ey][fy] * Gz[ez][fz];
+        const R t = Gx[ex][fx] * Gy[ey][fy] * Gz[ez][fz];
         if constexpr (wt(K) == 0)
             at<K>(A, e, f) += t;
         else if constexpr (wt(K) == 1)
@@ -296,12 +300,11 @@ struct Cls {
             at<K>(A, e, f) = fma(b2, t, at<K>(A, e, f));
     }
     template <int K, int... Js>
-    __device__ __forceinline__ static void acc_arr(Acc& A, const GtX& Gx, const GtY& Gy, const GtZ& Gz, double a2,
-                                                   double b2, std::integer_sequence<int, Js...>) {
+    __device__ __forceinline__ static void acc_arr(Acc& A, const GtX& Gx, const GtY& Gy, const GtZ& Gz, R a2, R b2,
+                                                   std::integer_sequence<int, Js...>) {
         (acc_one<K, Js>(A, Gx, Gy, Gz, a2, b2), ...);
     }
-    __device__ __forceinline__ static void acc_all(Acc& A, const GtX& Gx, const GtY& Gy, const GtZ& Gz, double a2,
-                                                   double b2) {
+    __device__ __forceinline__ static void acc_all(Acc& A, const GtX& Gx, const GtY& Gy, const GtZ& Gz, R a2, R b2) {
         acc_arr<0>(A, Gx, Gy, Gz, a2, b2, std::make_integer_sequence<int, ne(0) * NL>{});
         if constexpr (NARR > 1) acc_arr<1>(A, Gx, Gy, Gz, a2, b2, std::make_integer_sequence<int, ne(1) * NL>{});
         if constexpr (NARR > 2) acc_arr<2>(A, Gx, Gy, Gz, a2, b2, std::make_integer_sequence<int, ne(2) * NL>{});
@@ -310,15 +313,15 @@ struct Cls {
 #pragma unroll
         for (int e = 0; e < NE0; ++e)
 #pragma unroll
-            for (int f = 0; f < NL; ++f) A.a0[e][f] = 0.0;
+            for (int f = 0; f < NL; ++f) A.a0[e][f] = R(0);
 #pragma unroll
         for (int e = 0; e < NE1; ++e)
 #pragma unroll
-            for (int f = 0; f < NL; ++f) A.a1[e][f] = 0.0;
+            for (int f = 0; f < NL; ++f) A.a1[e][f] = R(0);
 #pragma unroll
         for (int e = 0; e < NE2; ++e)
 #pragma unroll
-            for (int f = 0; f < NL; ++f) A.a2[e][f] = 0.0;
+            for (int f = 0; f < NL; ++f) A.a2[e][f] = R(0);
     }
 
     template <int N, int K>
@@ -421,6 +424,7 @@ struct Cls {
 
 template <class CL>
 __device__ __forceinline__ void rys_thread_body(const TmplArgs& g, long task, double* sgrad) {
+    using R = typename CL::R;
     constexpr int NR = CL::NR, NM = CL::NM, LB = CL::LB;
     // per-thread root slot after the optional gradient buffer
     extern __shared__ double smem_all[];
@@ -452,8 +456,8 @@ __device__ __forceinline__ void rys_thread_body(const TmplArgs& g, long task, do
     for (int iab = 0; iab < nab; ++iab) {
         const double p = g.ps.eta[p0 + iab];
         const double cK = g.ps.cK[p0 + iab];
-        const double a2 = CL::DERIV ? 2.0 * g.ps.ea[p0 + iab] : 0.0;
-        const double b2 = CL::DERIV ? 2.0 * g.ps.eb[p0 + iab] : 0.0;
+        const R a2 = CL::DERIV ? (R)(2.0 * g.ps.ea[p0 + iab]) : R(0);
+        const R b2 = CL::DERIV ? (R)(2.0 * g.ps.eb[p0 + iab]) : R(0);
         const double Pp[3] = {g.ps.Px[p0 + iab], g.ps.Py[p0 + iab], g.ps.Pz[p0 + iab]};
         double PA[3], CP[3], PQ2 = 0.0;
 #pragma unroll
@@ -493,9 +497,11 @@ __device__ __forceinline__ void rys_thread_body(const TmplArgs& g, long task, do
                 typename CL::GtX Gx;
                 typename CL::GtY Gy;
                 typename CL::GtZ Gz;
-                build_G_t<NM, CL::MDX>(Gx, pref * wu, PA[0] + qi * x * CP[0], -pi * x * CP[0], B0, B1, B1p);
-                build_G_t<NM, CL::MDY>(Gy, 1.0, PA[1] + qi * x * CP[1], -pi * x * CP[1], B0, B1, B1p);
-                build_G_t<NM, CL::MDZ>(Gz, 1.0, PA[2] + qi * x * CP[2], -pi * x * CP[2], B0, B1, B1p);
+                const R b0 = (R)B0, b1 = (R)B1, b1p = (R)B1p;
+                build_G_t<NM, CL::MDX, R>(Gx, (R)(pref * wu), (R)(PA[0] + qi * x * CP[0]), (R)(-pi * x * CP[0]), b0,
+                                          b1, b1p);
+                build_G_t<NM, CL::MDY, R>(Gy, R(1), (R)(PA[1] + qi * x * CP[1]), (R)(-pi * x * CP[1]), b0, b1, b1p);
+                build_G_t<NM, CL::MDZ, R>(Gz, R(1), (R)(PA[2] + qi * x * CP[2]), (R)(-pi * x * CP[2]), b0, b1, b1p);
                 CL::acc_all(acc, Gx, Gy, Gz, a2, b2);
             }
         }
@@ -552,7 +558,7 @@ __device__ __forceinline__ void rys_thread_body(const TmplArgs& g, long task, do
 #ifndef DFB_THREAD_MIN_BLOCKS
 #define DFB_THREAD_MIN_BLOCKS 1
 #endif
-template <int LA, int LB, int LC, int FS, bool DERIV, bool SPLIT, int MINB = 1>
+template <int LA, int LB, int LC, int FS, bool DERIV, bool SPLIT, int MINB = 1, typename R = double>
 __global__ void __launch_bounds__(128, (DFB_THREAD_MIN_BLOCKS > MINB ? DFB_THREAD_MIN_BLOCKS : MINB))
     k_rys_thread(TmplArgs g) {
     extern __shared__ double sgrad[];
@@ -568,9 +574,9 @@ __global__ void __launch_bounds__(128, (DFB_THREAD_MIN_BLOCKS > MINB ? DFB_THREA
 #define DFB_FSI(I)                                                                                              \
     case I:                                                                                                     \
         if constexpr (I < FS)                                                                                   \
-            rys_thread_body<Cls<LA, LB, LC, FS, (I < FS ? I : 0), M0>>(g, task, sgrad);                         \
+            rys_thread_body<Cls<LA, LB, LC, FS, (I < FS ? I : 0), M0, R>>(g, task, sgrad);                      \
         else if constexpr (SPLIT && I < 2 * FS)                                                                 \
-            rys_thread_body<Cls<LA, LB, LC, FS, (I >= FS && I < 2 * FS ? I - FS : 0), 3>>(g, task, sgrad);      \
+            rys_thread_body<Cls<LA, LB, LC, FS, (I >= FS && I < 2 * FS ? I - FS : 0), 3, R>>(g, task, sgrad);   \
         break;
             DFB_FSI(0) DFB_FSI(1) DFB_FSI(2) DFB_FSI(3) DFB_FSI(4) DFB_FSI(5) DFB_FSI(6) DFB_FSI(7)
             DFB_FSI(8) DFB_FSI(9) DFB_FSI(10) DFB_FSI(11) DFB_FSI(12) DFB_FSI(13) DFB_FSI(14) DFB_FSI(15)

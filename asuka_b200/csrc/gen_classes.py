@@ -1,11 +1,12 @@
 """Generate the class-specialised Rys kernel instantiations (dfb_cls_*.cu).
 
-For every angular class (la >= lb, lc) and both variants (integrals,
-derivative contraction) this picks the smallest split FS of the aux shell's
+For every angular class (la >= lb, lc), both variants (integrals, derivative
+contraction) and both component types (FP64, and the mixed-precision float
+tables/accumulators) this picks the smallest split FS of the aux shell's
 Cartesian components such that one thread's accumulators fit the register
-budget, and emits an instantiation of ``k_rys_thread<LA, LB, LC, FS, DERIV>``
+budget, and emits an instantiation of ``k_rys_thread<LA, LB, LC, FS, DERIV, ...>``
 with a dispatcher.  Classes that do not fit stay on the generic warp kernel.
-One output file per (variant, la) so the files compile in parallel.
+One output file per (variant, type, la, lb) so the files compile in parallel.
 
     python asuka_b200/csrc/gen_classes.py
 """
@@ -63,19 +64,24 @@ def _key(la, lb, lc, deriv):
     return f"{'d' if deriv else 'i'}{la}{lb}{lc}"
 
 
-def plan(la, lb, lc, deriv, budget=None):
+def plan(la, lb, lc, deriv, budget=None, f32=False):
     """(FS, SPLIT) for a class, or None when it stays on the generic warp kernel.
 
     ``budget`` overrides the accumulator budget; without it the measured per-class table
     (``class_tuning.json``, "acc_budget") or the default ACC_BUDGET applies.  The
     environment variable DFB_GEN_ACC_BUDGET_DERIV sets the derivative default (the tuner's
-    variant builds) and DFB_GEN_ACC_BUDGET_INT the integral one.
+    variant builds) and DFB_GEN_ACC_BUDGET_INT the integral one.  Budgets count doubles;
+    the mixed-precision kernels (``f32``) hold float accumulators and recurrence tables, so
+    the same registers hold twice as many elements.
     """
     if budget is None:
         budget = tuning("acc_budget").get(_key(la, lb, lc, deriv))
     if budget is None:
         env = os.environ.get("DFB_GEN_ACC_BUDGET_DERIV" if deriv else "DFB_GEN_ACC_BUDGET_INT")
         budget = int(env) if env else ACC_BUDGET[deriv]
+    gbudget = G_BUDGET
+    if f32:
+        budget, gbudget = 2 * budget, 2 * G_BUDGET
     nm = la + lb + (1 if deriv else 0)
     nf = ncart(lc)
     modes = [(1, False), (None, True)] if deriv else [(0, False)]
@@ -85,7 +91,7 @@ def plan(la, lb, lc, deriv, budget=None):
             nfs = -(-nf // fs)
             if -(-nf // nfs) != fs:
                 continue  # keep the split exact (no empty subsets)
-            if per_f * nfs <= budget and g_cost(nm, lc, nfs) <= G_BUDGET:
+            if per_f * nfs <= budget and g_cost(nm, lc, nfs) <= gbudget:
                 return fs, split
     return None
 
@@ -103,63 +109,68 @@ def tuning(field: str = "min_blocks") -> dict:
         return json.load(f).get(field, {})
 
 
+def _groups():
+    """Files of the generated set: one per (variant, precision, la, lb) so they compile in parallel."""
+    out = []
+    for deriv in (False, True):
+        for f32 in (False, True):
+            for la in range(LA_MAX + 1):
+                for lb in range(la + 1):
+                    cls = [(la, lb, lc, *pl) for lc in range(LC_MAX + 1)
+                           if (pl := plan(la, lb, lc, deriv, f32=f32)) is not None]
+                    if cls:
+                        out.append((f"dfb_cls_{'d' if deriv else 'i'}{'f' if f32 else ''}{la}{lb}", deriv, f32, la, lb,
+                                    cls))
+    return out
+
+
 def main() -> None:
     tune = tuning()
     for old in os.listdir(HERE):
         if old.startswith("dfb_cls_") and old.endswith(".cu"):
             os.remove(os.path.join(HERE, old))
-    groups = []
-    for deriv in (False, True):
-        for la in range(LA_MAX + 1):
-            cls = []
-            for lb in range(la + 1):
-                for lc in range(LC_MAX + 1):
-                    pl = plan(la, lb, lc, deriv)
-                    if pl is not None:
-                        cls.append((la, lb, lc, *pl))
-            if not cls:
-                continue
-            name = f"dfb_cls_{'d' if deriv else 'i'}{la}"
-            groups.append(name)
-            lines = [
-                "// Generated by gen_classes.py -- class-specialised Rys kernel instantiations.",
-                '#include "dfb_rys_tmpl.cuh"',
-                "",
-                "namespace dfb {",
-                f"int {name}_launch(int la, int lb, int lc, const TmplArgs& g, long nblk, size_t smem, cudaStream_t st) {{",
-                "    (void)la;",
-            ]
-            for (a, b, c, fs, split) in cls:
-                minb = int(tune.get(_key(a, b, c, deriv), 1))
-                kern = (f"k_rys_thread<{a}, {b}, {c}, {fs}, {'true' if deriv else 'false'}, "
-                        f"{'true' if split else 'false'}, {minb}>")
-                lines.append(f"    if (lb == {b} && lc == {c}) {{")
-                lines.append(f"        {kern}<<<dim3((unsigned)nblk, {fs * (2 if split else 1)}), 128, smem, st>>>(g);")
-                lines.append("        return 1;")
-                lines.append("    }")
-            lines += ["    return 0;", "}", "}  // namespace dfb", ""]
-            with open(os.path.join(HERE, name + ".cu"), "w") as f:
-                f.write("\n".join(lines))
+    groups = _groups()
+    for name, deriv, f32, la, lb, cls in groups:
+        lines = [
+            "// Generated by gen_classes.py -- class-specialised Rys kernel instantiations.",
+            '#include "dfb_rys_tmpl.cuh"',
+            "",
+            "namespace dfb {",
+            f"int {name}_launch(int lc, const TmplArgs& g, long nblk, size_t smem, cudaStream_t st) {{",
+        ]
+        for (a, b, c, fs, split) in cls:
+            minb = 1 if f32 else int(tune.get(_key(a, b, c, deriv), 1))
+            kern = (f"k_rys_thread<{a}, {b}, {c}, {fs}, {'true' if deriv else 'false'}, "
+                    f"{'true' if split else 'false'}, {minb}, {'float' if f32 else 'double'}>")
+            lines.append(f"    if (lc == {c}) {{")
+            lines.append(f"        {kern}<<<dim3((unsigned)nblk, {fs * (2 if split else 1)}), 128, smem, st>>>(g);")
+            lines.append("        return 1;")
+            lines.append("    }")
+        lines += ["    return 0;", "}", "}  // namespace dfb", ""]
+        with open(os.path.join(HERE, name + ".cu"), "w") as f:
+            f.write("\n".join(lines))
     # dispatcher header
     hdr = ["// Generated by gen_classes.py -- dispatch over the class-specialised kernels.", "#pragma once",
            '#include "dfb_rys_tmpl.cuh"', "", "namespace dfb {"]
-    for name in groups:
-        hdr.append(f"int {name}_launch(int la, int lb, int lc, const TmplArgs& g, long nblk, size_t smem, cudaStream_t st);")
-    hdr += ["", "inline int tmpl_launch(int la, int lb, int lc, bool deriv, const TmplArgs& g, long nblk, size_t smem,",
-            "                       cudaStream_t st) {"]
-    for name in groups:
-        d = name[8] == "d"
-        la = int(name[9:])
-        hdr.append(f"    if ({'deriv' if d else '!deriv'} && la == {la}) return {name}_launch(la, lb, lc, g, nblk, smem, st);")
+    for name, *_ in groups:
+        hdr.append(f"int {name}_launch(int lc, const TmplArgs& g, long nblk, size_t smem, cudaStream_t st);")
+    hdr += ["", "// f32: the mixed-precision variant (float recurrence tables and accumulators)",
+            "inline int tmpl_launch(int la, int lb, int lc, bool deriv, bool f32, const TmplArgs& g, long nblk,",
+            "                       size_t smem, cudaStream_t st) {"]
+    for name, deriv, f32, la, lb, _cls in groups:
+        hdr.append(f"    if ({'deriv' if deriv else '!deriv'} && {'f32' if f32 else '!f32'} && la == {la} && lb == {lb})"
+                   f" return {name}_launch(lc, g, nblk, smem, st);")
     hdr += ["    return 0;", "}", ""]
     # host-side query: is a class served by a specialised kernel?
-    hdr.append("inline bool tmpl_has(int la, int lb, int lc, bool deriv) {")
+    hdr.append("inline bool tmpl_has(int la, int lb, int lc, bool deriv, bool f32) {")
     for deriv in (False, True):
-        keys = [f"({la}, {lb}, {lc})" for la in range(LA_MAX + 1) for lb in range(la + 1) for lc in range(LC_MAX + 1)
-                if plan(la, lb, lc, deriv) is not None]
-        hdr.append(f"    static const int k{'d' if deriv else 'i'}[][3] = {{{', '.join('{' + k[1:-1] + '}' for k in keys)}}};")
-    hdr += ["    const int (*k)[3] = deriv ? kd : ki;",
-            "    const int n = deriv ? (int)(sizeof(kd) / sizeof(kd[0])) : (int)(sizeof(ki) / sizeof(ki[0]));",
+        for f32 in (False, True):
+            keys = [f"{{{la}, {lb}, {lc}}}" for la in range(LA_MAX + 1) for lb in range(la + 1)
+                    for lc in range(LC_MAX + 1) if plan(la, lb, lc, deriv, f32=f32) is not None]
+            hdr.append(f"    static const int k{'d' if deriv else 'i'}{'f' if f32 else ''}[][3] = {{{', '.join(keys)}}};")
+    hdr += ["    const int (*k)[3] = deriv ? (f32 ? kdf : kd) : (f32 ? kif : ki);",
+            "    const int n = deriv ? (f32 ? (int)(sizeof(kdf) / sizeof(kdf[0])) : (int)(sizeof(kd) / sizeof(kd[0])))",
+            "                        : (f32 ? (int)(sizeof(kif) / sizeof(kif[0])) : (int)(sizeof(ki) / sizeof(ki[0])));",
             "    for (int i = 0; i < n; ++i)",
             "        if (k[i][0] == la && k[i][1] == lb && k[i][2] == lc) return true;",
             "    return false;", "}", "}  // namespace dfb", ""]

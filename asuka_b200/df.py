@@ -91,6 +91,46 @@ def ensure_rys_table(device: torch.device) -> None:
     _TABLE_READY.add(idx)
 
 
+PREC_FP64, PREC_MIXED = 0, 1  # DFB_PREC_FP64 / DFB_PREC_MIXED of include/dfb.h
+PREC_ALL_MIXED = -1  # 'mixed_all': every class in FP32 (measurement of the per-class errors)
+
+
+def _prec_code(precision: str) -> int:
+    """'fp64' -> DFB_PREC_FP64; 'mixed' -> DFB_PREC_MIXED for the classes the precision table
+    admits (FP64 for the others); 'mixed_all' -> DFB_PREC_MIXED for every class."""
+    if precision == "fp64":
+        return PREC_FP64
+    if precision == "mixed":
+        return PREC_MIXED
+    if precision == "mixed_all":
+        return PREC_ALL_MIXED
+    raise ValueError(f"precision must be 'fp64', 'mixed' or 'mixed_all', got {precision!r}")
+
+
+@functools.lru_cache(maxsize=1)
+def mixed_class_table() -> dict:
+    """Angular classes whose FP32-component kernels the mixed mode uses, per kind ('int3c',
+    'deriv3c', 'deriv2c'), as sets of (la, lb, lc).  Written by ``asuka_b200.tune_precision``
+    from the measured first-order energy and gradient errors of every class (FP32 against FP64
+    kernels); classes not listed run in FP64 in mixed mode too."""
+    p = os.path.join(_DATA, "class_precision.json")
+    if not os.path.exists(p):
+        return {}
+    import json
+
+    with open(p) as f:
+        t = json.load(f)
+    return {k: {tuple(int(v) for v in c) for c in t.get(k, [])} for k in ("int3c", "deriv3c", "deriv2c")}
+
+
+def _class_prec(code: int, kind: str, la: int, lb: int, lc: int) -> int:
+    if code == PREC_FP64:
+        return PREC_FP64
+    if code == PREC_ALL_MIXED:
+        return PREC_MIXED
+    return PREC_MIXED if (la, lb, lc) in mixed_class_table().get(kind, ()) else PREC_FP64
+
+
 def _stream() -> int:
     return int(torch.cuda.current_stream().cuda_stream)
 
@@ -355,7 +395,7 @@ class DFEngine:
         return blocks
 
     def int3c_block(self, blk, p0: int, p1: int, out: torch.Tensor | None = None,
-                    dropped_zero: bool = False) -> torch.Tensor:
+                    dropped_zero: bool = False, precision: str = "fp64") -> torch.Tensor:
         """X rows for one aux block as (p1-p0, nao, nao) (streamed DF, ``gpu.py:2742``).
 
         Entries of screened-out shell pairs are not written; they are zeroed here
@@ -377,11 +417,11 @@ class DFEngine:
             seen.add((la, lb, lc))
             auxs = byl[lc]
             launches.append(self._launch_int(la, lb, lc, self.ps_ao, axb, pairs, auxs, pairs.numel() * auxs.numel(),
-                                             -pairs.numel(), 0, X, (nao * nao, nao, 1)))
+                                             -pairs.numel(), 0, X, (nao * nao, nao, 1), _prec_code(precision)))
         self._fanout(launches)
         return X
 
-    def deriv3c_block(self, blk, bar: torch.Tensor, grad: torch.Tensor) -> torch.Tensor:
+    def deriv3c_block(self, blk, bar: torch.Tensor, grad: torch.Tensor, precision: str = "fp64") -> torch.Tensor:
         """grad += sum over one aux block of bar[P-p0, mu, nu] d(mu nu|P)/dR (block-local adjoint)."""
         axb, _shifted, byl = blk
         nao = self.nao
@@ -395,7 +435,8 @@ class DFEngine:
             seen.add((la, lb, lc))
             auxs = byl[lc]
             launches.append(self._launch_deriv(la, lb, lc, self.ps_ao, axb, pairs, auxs, pairs.numel() * auxs.numel(),
-                                               -pairs.numel(), 0, bar, (nao * nao, nao, 1), grad))
+                                               -pairs.numel(), 0, bar, (nao * nao, nao, 1), grad,
+                                               _prec_code(precision)))
         self._fanout(launches)
         return grad
 
@@ -406,28 +447,32 @@ class DFEngine:
         per = buf.numel() // n
         return [buf[i * per:(i + 1) * per] for i in range(n)]
 
-    def _launch_int(self, la, lb, lc, ps, axs, pairs, auxs, ntask, ngrid, mode, out, strides):
+    def _launch_int(self, la, lb, lc, ps, axs, pairs, auxs, ntask, ngrid, mode, out, strides, prec=PREC_FP64):
         L = _lib.lib()
-        key = (la, lb, lc, mode)
+        # the metric (mode 1) stays FP64: its Cholesky factor whitens everything downstream
+        prec = PREC_FP64 if mode == 1 else _class_prec(prec, "int3c", la, lb, lc)
+        key = (la, lb, lc, mode, prec)
 
         def fn(stream, _k=key):
             i = self._slot_of(stream)
             scr = self._slices_int[i]
-            rc = L.dfb_rys_int(la, lb, lc, ctypes.byref(ps), ctypes.byref(axs), _lib.ptr(pairs), _lib.ptr(auxs),
-                               ntask, ngrid, mode, _lib.ptr(out), *strides, _lib.ptr(scr), scr.numel(), stream)
+            rc = L.dfb_rys_int_prec(la, lb, lc, ctypes.byref(ps), ctypes.byref(axs), _lib.ptr(pairs), _lib.ptr(auxs),
+                                    ntask, ngrid, mode, prec, _lib.ptr(out), *strides, _lib.ptr(scr), scr.numel(),
+                                    stream)
             _lib.check(rc, f"dfb_rys_int {_k}")
         return fn
 
-    def _launch_deriv(self, la, lb, lc, ps, axs, pairs, auxs, ntask, ngrid, mode, bar, strides, grad):
+    def _launch_deriv(self, la, lb, lc, ps, axs, pairs, auxs, ntask, ngrid, mode, bar, strides, grad, prec=PREC_FP64):
         L = _lib.lib()
-        key = (la, lb, lc, mode)
+        prec = _class_prec(prec, "deriv2c" if mode == 1 else "deriv3c", la, lb, lc)
+        key = (la, lb, lc, mode, prec)
 
         def fn(stream, _k=key):
             i = self._slot_of(stream)
             scr = self._slices_der[i]
-            rc = L.dfb_rys_deriv(la, lb, lc, ctypes.byref(ps), ctypes.byref(axs), _lib.ptr(pairs), _lib.ptr(auxs),
-                                 ntask, ngrid, mode, _lib.ptr(bar), *strides, _lib.ptr(grad), self.natm,
-                                 _lib.ptr(scr), scr.numel(), stream)
+            rc = L.dfb_rys_deriv_prec(la, lb, lc, ctypes.byref(ps), ctypes.byref(axs), _lib.ptr(pairs),
+                                      _lib.ptr(auxs), ntask, ngrid, mode, prec, _lib.ptr(bar), *strides,
+                                      _lib.ptr(grad), self.natm, _lib.ptr(scr), scr.numel(), stream)
             _lib.check(rc, f"dfb_rys_deriv {_k}")
         return fn
 
@@ -452,8 +497,11 @@ class DFEngine:
         V.copy_(0.5 * (V + V.T))
         return V
 
-    def int3c(self, layout: str = "Qmn", out: torch.Tensor | None = None) -> torch.Tensor:
-        """X = (mu nu|P): 'Qmn' -> (naux, nao, nao), 'mnQ' -> (nao, nao, naux)."""
+    def int3c(self, layout: str = "Qmn", out: torch.Tensor | None = None, precision: str = "fp64") -> torch.Tensor:
+        """X = (mu nu|P): 'Qmn' -> (naux, nao, nao), 'mnQ' -> (nao, nao, naux).
+
+        ``precision='mixed'`` runs the class kernels with FP32 recurrence tables and
+        accumulators (``DFB_PREC_MIXED``); the output stays FP64."""
         nao, naux = self.nao, self.naux
         if layout == "Qmn":
             shape, s = (naux, nao, nao), (nao * nao, nao, 1)
@@ -465,11 +513,12 @@ class DFEngine:
         if self.n_dropped_pairs:
             X.zero_()
         self._slices_int = self._scratch_slices(False)
+        pc = _prec_code(precision)
         self._fanout([self._launch_int(la, lb, lc, self.ps_ao, self.axs, pairs, auxs, pairs.numel() * auxs.numel(),
-                                       -pairs.numel(), 0, X, s) for la, lb, lc, pairs, auxs in self.classes3c])
+                                       -pairs.numel(), 0, X, s, pc) for la, lb, lc, pairs, auxs in self.classes3c])
         return X
 
-    def deriv3c(self, bar: torch.Tensor, grad: torch.Tensor, layout: str = "Qmn") -> torch.Tensor:
+    def deriv3c(self, bar: torch.Tensor, grad: torch.Tensor, layout: str = "Qmn", precision: str = "fp64") -> torch.Tensor:
         """grad += sum_{mu nu P} bar[mu nu P] d(mu nu|P)/dR; bar symmetric in (mu, nu)."""
         nao, naux = self.nao, self.naux
         if layout == "Qmn":
@@ -480,22 +529,25 @@ class DFEngine:
             raise ValueError("layout must be 'Qmn' or 'mnQ'")
         bar = bar.contiguous()
         self._slices_der = self._scratch_slices(True)
+        pc = _prec_code(precision)
         self._fanout([self._launch_deriv(la, lb, lc, self.ps_ao, self.axs, pairs, auxs, pairs.numel() * auxs.numel(),
-                                         -pairs.numel(), 0, bar, s, grad) for la, lb, lc, pairs, auxs in self.classes3c])
+                                         -pairs.numel(), 0, bar, s, grad, pc)
+                      for la, lb, lc, pairs, auxs in self.classes3c])
         return grad
 
-    def deriv2c(self, bar: torch.Tensor, grad: torch.Tensor) -> torch.Tensor:
+    def deriv2c(self, bar: torch.Tensor, grad: torch.Tensor, precision: str = "fp64") -> torch.Tensor:
         """grad += sum_{P,Q} bar[P,Q] d(P|Q)/dR; bar symmetric."""
         naux = self.naux
         bar = bar.contiguous()
         self._slices_der = self._scratch_slices(True)
+        pc = _prec_code(precision)
         self._fanout([self._launch_deriv(lp, 0, lq, self.ps_aux, self.axs, P, Q, P.numel(), 0, 1, bar, (naux, 1, 0),
-                                         grad) for lp, lq, P, Q in self.classes2c])
+                                         grad, pc) for lp, lq, P, Q in self.classes2c])
         return grad
 
 
     # ------------------------------------------------------------ overlapped phases of one step
-    def metric_cholesky_int3c(self, X: torch.Tensor | None = None):
+    def metric_cholesky_int3c(self, X: torch.Tensor | None = None, precision: str = "fp64"):
         """V = (P|Q), its Cholesky factor L and X = (mu nu|P) ('Qmn') with the phases overlapped.
 
         The metric classes go to the side streams first and the 3c classes after them; the
@@ -506,7 +558,7 @@ class DFEngine:
         nao, naux = self.nao, self.naux
         if NSTREAMS <= 1:
             V = self.metric()
-            return V, cholesky_metric(V), self.int3c("Qmn", out=X)
+            return V, cholesky_metric(V), self.int3c("Qmn", out=X, precision=precision)
         V = torch.empty((naux, naux), dtype=torch.float64, device=self.device)
         X = X if X is not None else torch.empty((naux, nao, nao), dtype=torch.float64, device=self.device)
         if self.n_dropped_pairs:
@@ -514,8 +566,9 @@ class DFEngine:
         self._slices_int = self._scratch_slices(False)
         first = [self._launch_int(lp, 0, lq, self.ps_aux, self.axs, P, Q, P.numel(), 0, 1, V, (naux, 1, 0))
                  for lp, lq, P, Q in self.classes2c]
+        pc = _prec_code(precision)
         second = [self._launch_int(la, lb, lc, self.ps_ao, self.axs, pairs, auxs, pairs.numel() * auxs.numel(),
-                                   -pairs.numel(), 0, X, (nao * nao, nao, 1))
+                                   -pairs.numel(), 0, X, (nao * nao, nao, 1), pc)
                   for la, lb, lc, pairs, auxs in self.classes3c]
         main = torch.cuda.current_stream(self.device)
         side = self._streams()
@@ -541,17 +594,19 @@ class DFEngine:
             raise RuntimeError(f"metric Cholesky failed (leading minor {int(info.item())} not positive definite)")
         return V, L, X
 
-    def deriv3c_2c(self, bar3: torch.Tensor, bar2: torch.Tensor, grad: torch.Tensor) -> torch.Tensor:
+    def deriv3c_2c(self, bar3: torch.Tensor, bar2: torch.Tensor, grad: torch.Tensor,
+                   precision: str = "fp64") -> torch.Tensor:
         """deriv3c(bar3 'Qmn') and deriv2c(bar2) as one fan-out (both add into grad atomically)."""
         nao, naux = self.nao, self.naux
         bar3 = bar3.contiguous()
         bar2 = bar2.contiguous()
         self._slices_der = self._scratch_slices(True)
+        pc = _prec_code(precision)
         launches = [self._launch_deriv(la, lb, lc, self.ps_ao, self.axs, pairs, auxs, pairs.numel() * auxs.numel(),
-                                       -pairs.numel(), 0, bar3, (nao * nao, nao, 1), grad)
+                                       -pairs.numel(), 0, bar3, (nao * nao, nao, 1), grad, pc)
                     for la, lb, lc, pairs, auxs in self.classes3c]
         launches += [self._launch_deriv(lp, 0, lq, self.ps_aux, self.axs, P, Q, P.numel(), 0, 1, bar2, (naux, 1, 0),
-                                        grad) for lp, lq, P, Q in self.classes2c]
+                                        grad, pc) for lp, lq, P, Q in self.classes2c]
         self._fanout(launches)
         return grad
 

@@ -31,7 +31,18 @@ import torch
 
 from . import linalg as _la
 from . import mixed as _mixed
+from . import tc as _tc
 from .df import DFEngine, cholesky_metric
+
+# Mixed mode: which dense products run as split-BF16 tensor-core GEMMs (tcgen05, three terms).
+# The tensor cores' FP32 accumulation is biased (it truncates), about 1e-7 relative in the same
+# direction for every element, and a bias does not average out: run as a tensor-core product,
+# Y = X Cw moved E_2e of (H2O)8 by 4e-4 Eh and Gamma moved the gradient by 2e-6 Eh/bohr.  So only
+# the exchange update K = sum W W^T runs there by default: it enters neither the energy (taken
+# from M = Cw^T W in FP64) nor the gradient, only the Fock matrix of the early SCF iterations.
+MIXED_K_TC = True
+MIXED_Y_TC = False
+MIXED_GAMMA_TC = False
 
 
 def _mm(A, B, precision):
@@ -44,7 +55,7 @@ def _nomark(_key: str) -> None:
 
 def df_forward(engine: DFEngine, Cw: torch.Tensor, precision: str = "fp64", X: torch.Tensor | None = None):
     """Integrals at the engine's current geometry, then (E_2e, J, K) and the saved intermediates."""
-    _V, L, X = engine.metric_cholesky_int3c(X)
+    _V, L, X = engine.metric_cholesky_int3c(X, precision=precision)
     return df_contract(engine, Cw, X, L, precision)
 
 
@@ -58,10 +69,14 @@ def df_contract(engine: DFEngine, Cw: torch.Tensor, X: torch.Tensor, L: torch.Te
     """
     nao, naux = engine.nao, engine.naux
     nocc = Cw.shape[1]
+    mixed = precision != "fp64"
     X2 = X.view(naux, nao * nao)
     D = Cw @ Cw.T
     D = 0.5 * (D + D.T)
-    Y = (X.view(naux * nao, nao) @ Cw).view(naux, nao * nocc)
+    if mixed and MIXED_Y_TC:
+        Y = _tc.matmul(X.view(naux * nao, nao), Cw).view(naux, nao * nocc)
+    else:
+        Y = (X.view(naux * nao, nao) @ Cw).view(naux, nao * nocc)
     mark("jk_Y")
     rho = Y @ Cw.reshape(-1)
     d = torch.cholesky_solve(rho.view(-1, 1), L).view(-1)
@@ -73,21 +88,30 @@ def df_contract(engine: DFEngine, Cw: torch.Tensor, X: torch.Tensor, L: torch.Te
     Linv_blocks = _la.diag_block_inverses(L)
     W = _la.solve_lower(L, Y, Linv_blocks, out=Y)
     mark("jk_W_solve")
-    W2 = W.view(naux, nao, nocc).permute(1, 0, 2).reshape(nao, naux * nocc)
-    K = _mixed.syrk(W2) if (precision != "fp64" and nao >= _mixed.MIN_DIM) else W2 @ W2.T
+    W3 = W.view(naux, nao, nocc)
+    # M_Q = Cw^T W_Q (FP64 in both modes): the exchange energy tr(D K) = sum_Q |M_Q|^2, and the
+    # adjoint's input
+    M = torch.matmul(Cw.T, W3)
+    if mixed and MIXED_K_TC:
+        K = _tc.syrk_qblocks(W3)
+    else:
+        W2 = W3.permute(1, 0, 2).reshape(nao, naux * nocc)
+        K = W2 @ W2.T
     K = 0.5 * (K + K.T)
-    E = 0.5 * torch.dot(rho, d) - 0.25 * torch.sum(D * K)
+    E = 0.5 * torch.dot(rho, d) - 0.25 * torch.sum(M * M)
     mark("jk_K")
-    return E, J, K, dict(X=X, L=L, d=d, W=W, D=D, Linv_blocks=Linv_blocks)
+    return E, J, K, dict(X=X, L=L, d=d, W=W, M=M, D=D, Linv_blocks=Linv_blocks)
 
 
-def df_adjoints(engine: DFEngine, Cw: torch.Tensor, saved: dict):
+def df_adjoints(engine: DFEngine, Cw: torch.Tensor, saved: dict, precision: str = "fp64"):
     """Adjoints of the 3c and 2c integrals: (Gamma (naux, nao, nao), written over X; G2 (naux, naux))."""
     nao, naux = engine.nao, engine.naux
     nocc = Cw.shape[1]
     X, L, d, W = saved["X"], saved["L"], saved["d"], saved["W"]
     # M_Q = Cw^T W_Q  (naux, nocc, nocc)
-    M = torch.matmul(Cw.T, W.view(naux, nao, nocc))
+    M = saved.get("M")
+    if M is None:
+        M = torch.matmul(Cw.T, W.view(naux, nao, nocc))
     M = 0.5 * (M + M.transpose(1, 2))
     Z = _la.solve_lower_T(L, M.reshape(naux, nocc * nocc), saved.get("Linv_blocks"))
     Zq = Z.view(naux, nocc, nocc)
@@ -96,7 +120,10 @@ def df_adjoints(engine: DFEngine, Cw: torch.Tensor, saved: dict):
     Zp = -0.5 * Zq + d.view(naux, 1, 1) * torch.eye(nocc, dtype=Zq.dtype, device=Zq.device)
     T = torch.matmul(Zp, Cw.T)  # (naux, nocc, nao)
     G3 = X
-    torch.matmul(Cw, T, out=G3)
+    if precision != "fp64" and MIXED_GAMMA_TC:
+        _tc.bmm(Cw, T, out=G3)
+    else:
+        torch.matmul(Cw, T, out=G3)
     G2 = -0.5 * torch.outer(d, d) + 0.25 * (Z @ Z.T)
     return G3, G2
 
@@ -104,10 +131,10 @@ def df_adjoints(engine: DFEngine, Cw: torch.Tensor, saved: dict):
 def df_backward(engine: DFEngine, Cw: torch.Tensor, saved: dict, grad: torch.Tensor | None = None,
                 precision: str = "fp64") -> torch.Tensor:
     """dE_2e/dR accumulated into grad (natm, 3)."""
-    G3, G2 = df_adjoints(engine, Cw, saved)
+    G3, G2 = df_adjoints(engine, Cw, saved, precision)
     if grad is None:
         grad = torch.zeros((engine.natm, 3), dtype=torch.float64, device=G3.device)
-    engine.deriv3c_2c(G3, G2, grad)
+    engine.deriv3c_2c(G3, G2, grad, precision=precision)
     return grad
 
 
@@ -141,16 +168,19 @@ def df_energy(coords: torch.Tensor, Cw: torch.Tensor, engine: DFEngine, precisio
 
 # ---------------------------------------------------------------- streamed (B never stored)
 
-def _solve_lower_inplace(L: torch.Tensor, Y: torch.Tensor, precision: str, ncol: int = 1 << 18) -> torch.Tensor:
+def _solve_lower_inplace(L: torch.Tensor, Y: torch.Tensor, mixed_solve: bool = False,
+                         ncol: int = 1 << 18) -> torch.Tensor:
     """Y <- L^-1 Y in place.
 
-    FP64: block substitution (``asuka_b200.linalg``).  Mixed: L^-1 formed once in
-    FP64, split once into BF16 terms, and applied to each column block as a
-    split-BF16 GEMM (one block copy alive at a time).
+    Default: FP64 block substitution (``asuka_b200.linalg``) -- the metric solve stays FP64
+    in every precision mode.  ``mixed_solve``: L^-1 formed once in FP64, split once into BF16
+    terms, and applied to each column block as a split-BF16 GEMM (one block copy alive at a
+    time); its error grows with the metric's condition number (1e-4 relative in K for the
+    ma-QZVP/RICD aux basis), so it is an explicit opt-in.
     """
     n, m = Y.shape
     ncol = max(1, min(m, ncol * 1024 // max(n, 1)))
-    if precision == "fp64":
+    if not mixed_solve:
         return _la.solve_lower(L, Y, out=Y)
     Linv = torch.linalg.solve_triangular(L, torch.eye(n, dtype=L.dtype, device=L.device), upper=False)
     sp = _mixed.split3(Linv)
@@ -162,7 +192,7 @@ def _solve_lower_inplace(L: torch.Tensor, Y: torch.Tensor, precision: str, ncol:
 
 
 def df_energy_grad_streamed(engine: DFEngine, Cw: torch.Tensor, aux_block: int = 128, precision: str = "fp64",
-                            stats: dict | None = None):
+                            stats: dict | None = None, mixed_solve: bool = False):
     """E_2e and dE_2e/dR without storing the 3c tensor: the integrals are recomputed per aux block.
 
     Forward: for each aux block b, X_b -> Y_b = X_b Cw (rho from Y); then d = V^-1 rho,
@@ -171,9 +201,10 @@ def df_energy_grad_streamed(engine: DFEngine, Cw: torch.Tensor, aux_block: int =
     block's derivative integrals (the streamed analogue of
     ``asuka/hf/df_jk_streamed.py:167-325``, with the gradient recomputing the integrals
     instead of reading a stored B).  The largest buffer is Y/W (naux x nao x nocc)
-    instead of the 3c tensor (naux x nao^2).  ``precision='mixed'`` runs the solve
-    W = L^-1 Y and the exchange update K as split-BF16 GEMMs (FP32 accumulation);
-    the integrals, the half-transforms and the adjoint stay FP64.
+    instead of the 3c tensor (naux x nao^2).  ``precision='mixed'`` evaluates the
+    integrals and their derivatives with FP32 recurrence tables and accumulators and
+    runs the exchange update K as a split-BF16 tensor-core GEMM; the metric solves stay
+    FP64 unless ``mixed_solve`` (split-BF16 product with L^-1) is asked for.
     Returns (E, grad (natm, 3), K).
     """
     nao, naux = engine.nao, engine.naux
@@ -190,21 +221,20 @@ def df_energy_grad_streamed(engine: DFEngine, Cw: torch.Tensor, aux_block: int =
     bmax = max(p1 - p0 for p0, p1, _ in blocks)
     Xb_buf = torch.zeros((bmax, nao, nao), dtype=torch.float64, device=dev)
     for p0, p1, blk in blocks:
-        Xb = engine.int3c_block(blk, p0, p1, out=Xb_buf[: p1 - p0], dropped_zero=True)
+        Xb = engine.int3c_block(blk, p0, p1, out=Xb_buf[: p1 - p0], dropped_zero=True, precision=precision)
         torch.matmul(Xb.view(-1, nao), Cw, out=Y[p0:p1].view(-1, nocc))
     ev[1].record()
     rho = Y @ Cw.reshape(-1)
     d = torch.cholesky_solve(rho.view(-1, 1), L).view(-1)
-    W = _solve_lower_inplace(L, Y, precision)
+    W = _solve_lower_inplace(L, Y, mixed_solve and precision != "fp64")
     W3 = W.view(naux, nao, nocc)
     K = torch.zeros((nao, nao), dtype=torch.float64, device=dev)
     qb = max(1, (1 << 27) // max(nao * nocc, 1))
-    for q0 in range(0, naux, qb):
+    if precision != "fp64":
+        _tc.syrk_qblocks(W3, out=K)  # reads W in place, k = (Q, i)
+    for q0 in range(0, naux if precision == "fp64" else 0, qb):
         Wc = W3[q0:q0 + qb].permute(1, 0, 2).reshape(nao, -1)
-        if precision == "fp64" or nao < _mixed.MIN_DIM:
-            K.addmm_(Wc, Wc.T)
-        else:
-            K += _mixed.syrk(Wc)
+        K.addmm_(Wc, Wc.T)
     K = 0.5 * (K + K.T)
     D = Cw @ Cw.T
     E = 0.5 * torch.dot(rho, d) - 0.25 * torch.sum(D * K)
@@ -225,10 +255,10 @@ def df_energy_grad_streamed(engine: DFEngine, Cw: torch.Tensor, aux_block: int =
         T = torch.matmul(Zp, Cw.T)
         G3 = Xb_buf[: p1 - p0]
         torch.matmul(Cw, T, out=G3)
-        engine.deriv3c_block(blk, G3, grad)
+        engine.deriv3c_block(blk, G3, grad, precision=precision)
     ev[4].record()
     G2 = -0.5 * torch.outer(d, d) + 0.25 * (Z @ Z.T)
-    engine.deriv2c(G2, grad)
+    engine.deriv2c(G2, grad, precision=precision)
     ev[5].record()
     if stats is not None:
         torch.cuda.synchronize(dev)
@@ -262,6 +292,26 @@ def whitened_adjoints(B: torch.Tensor, barL: torch.Tensor, L: torch.Tensor):
     return bar_X.contiguous(), (0.5 * (bar_V + bar_V.T)).contiguous()
 
 
+def whitened_adjoints_qp(B_Qp: torch.Tensor, barL_Qp: torch.Tensor, L: torch.Tensor, nao: int):
+    """``whitened_adjoints`` in the packed lower-triangle layout (naux, ntri), p = m(m+1)/2 + n.
+
+    Every step acts on the aux index or contracts over the full (mu, nu) square, which in packed
+    form is a weighted sum over p (weight 2 off the diagonal), so nothing is unpacked:
+    returns (bar_X in packed form (naux, ntri), bar_V (naux, naux)); the packed-Qp route of
+    ``asuka/integrals/df_grad_context.py:1160``.
+    """
+    naux = B_Qp.shape[0]
+    i, j = torch.tril_indices(nao, nao, device=B_Qp.device)
+    w = torch.where(i == j, 1.0, 2.0).to(torch.float64)
+    tmp = _la.solve_lower_T(L, barL_Qp)  # L^-T bar_B^T, packed (naux, ntri)
+    bar_Lc = -torch.tril((tmp * w) @ B_Qp.T)
+    G = torch.tril(L.T @ bar_Lc)
+    G.diagonal().mul_(0.5)
+    t2 = torch.linalg.solve_triangular(L.T, G, upper=True)
+    bar_V = torch.linalg.solve_triangular(L.T, t2.T, upper=True).T
+    return tmp, (0.5 * (bar_V + bar_V.T)).contiguous()
+
+
 def compute_df_gradient_contributions_analytic_packed_bases(ao_basis, aux_basis, *, atom_coords_bohr, B_ao,
                                                             bar_L_ao, L_chol=None, backend: str = "cuda",
                                                             df_threads: int = 0, profile: dict | None = None):
@@ -292,3 +342,38 @@ def compute_df_gradient_contributions_analytic_packed_bases(ao_basis, aux_basis,
     eng.deriv3c(bar_X, grad, layout="Qmn")
     eng.deriv2c(bar_V, grad)
     return grad.cpu().numpy()
+
+
+# ---------------------------------------------------------------- full RHF nuclear gradient
+
+def rhf_nuclear_gradient(res, precision: str = "fp64") -> np.ndarray:
+    """dE_RHF/dR (natm, 3) of a converged Cartesian DF-RHF result of ``scf.run_hf_df``.
+
+    Composed as the reference composes it (nuclear repulsion, ``contract_dhcore_cart`` with the
+    density, ``-contract_dS_cart`` with the energy-weighted density W = sum_i occ_i e_i C_i C_i^T,
+    and the DF two-electron gradient; ``asuka/integrals/int1e_cart.py:1452,1738``,
+    ``asuka/integrals/grad.py:114``), with the two-electron part from the Rys derivative kernels
+    through ``DFEnergyFunction`` at the converged orbitals.
+    """
+    from .int1e import contract_dhcore_cart, contract_dS_cart
+
+    mol = res.mol
+    ao = res.ao_basis
+    C = torch.as_tensor(res.mo_coeff, dtype=torch.float64)
+    occ = torch.as_tensor(res.mo_occ, dtype=torch.float64)
+    eps = torch.as_tensor(res.scf.mo_energy, dtype=torch.float64)
+    if C.shape[0] != ao.nao:
+        raise NotImplementedError("rhf_nuclear_gradient takes Cartesian-AO results (cart=True)")
+    Ch, occ_h, eps_h = C.cpu().numpy(), occ.cpu().numpy(), eps.cpu().numpy()
+    D = (Ch * occ_h) @ Ch.T
+    W = (Ch * (occ_h * eps_h)) @ Ch.T
+    R = np.asarray(mol.coords_bohr, dtype=np.float64)
+    g = mol.energy_nuc_grad() + contract_dhcore_cart(ao, atom_coords_bohr=R, atom_charges=mol.charges, M=D)
+    g = g - contract_dS_cart(ao, atom_coords_bohr=R, M=W)
+    eng = DFEngine(ao, res.aux_basis, atom_coords_bohr=R)
+    nocc = int((occ_h > 0).sum())
+    Cw = torch.as_tensor(Ch[:, :nocc] * np.sqrt(occ_h[:nocc]), device=eng.device).contiguous()
+    Rt = torch.as_tensor(R, device=eng.device).requires_grad_(True)
+    E2, _J, _K = df_energy(Rt, Cw, eng, precision)
+    (g2,) = torch.autograd.grad(E2, Rt)
+    return g + g2.cpu().numpy()

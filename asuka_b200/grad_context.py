@@ -9,7 +9,9 @@ contractions accept the layouts the reference hands over:
 * ``contract(B_ao, bar_L_ao)``: B in mnQ (nao, nao, naux) with dE/dB (naux, nao, nao), or
   both packed lower-triangle Qp (naux, ntri) with p = m(m+1)/2 + n (m >= n). Qp is the
   layout in which the DF SCF returns ``df_B``; both tensors hold the symmetric
-  full-layout values at their packed positions (``asuka/integrals/df_adjoint.py:238-321``);
+  full-layout values at their packed positions (``asuka/integrals/df_adjoint.py:238-321``).
+  The packed route never forms (naux, nao, nao): the adjoints are computed in packed form
+  and the derivative integrals run one aux-shell block at a time;
 * ``contract_sph(B_sph, bar_L_sph)``: spherical-AO factors. The adjoint is formed in the
   spherical basis and taken to the Cartesian integrals through the solid-harmonic
   transform, dE/dX_cart = T (dE/dX_sph) T^T;
@@ -27,7 +29,7 @@ import numpy as np
 import torch
 
 from .df import DFEngine, cholesky_metric
-from .grad import whitened_adjoints
+from .grad import whitened_adjoints, whitened_adjoints_qp
 
 
 def _nao_from_ntri(ntri: int) -> int:
@@ -37,14 +39,6 @@ def _nao_from_ntri(ntri: int) -> int:
     return nao
 
 
-def _unpack_Qp(Bqp: torch.Tensor, nao: int) -> torch.Tensor:
-    """(naux, ntri) -> (naux, nao, nao), symmetric."""
-    i = torch.arange(nao, device=Bqp.device)
-    hi = torch.maximum(i[:, None], i[None, :])
-    lo = torch.minimum(i[:, None], i[None, :])
-    return Bqp.index_select(1, (hi * (hi + 1) // 2 + lo).reshape(-1)).view(Bqp.shape[0], nao, nao)
-
-
 class DFGradContractionContext:
     def __init__(self, engine: DFEngine, L: torch.Tensor, natm: int):
         self.engine = engine
@@ -52,6 +46,7 @@ class DFGradContractionContext:
         self.backend = "cuda"
         self.nao, self.naux = engine.nao, engine.naux
         self.natm = max(engine.natm, natm)
+        self.last_peak_block_elems = 0  # largest unpacked (q, nao, nao) block of the last packed contraction
 
     @classmethod
     def build(cls, ao_basis: Any, aux_basis: Any, *, atom_coords_bohr: np.ndarray, backend: str = "cuda",
@@ -74,18 +69,7 @@ class DFGradContractionContext:
         self.L_metric = None
 
     # ------------------------------------------------------------ layouts
-    def _mnQ_and_bar(self, B_ao, bar_L_ao):
-        dev = self.engine.device
-        B = torch.as_tensor(B_ao, dtype=torch.float64, device=dev)
-        barL = torch.as_tensor(bar_L_ao, dtype=torch.float64, device=dev)
-        if B.ndim == 2 and barL.ndim == 2:  # packed Qp
-            naux, ntri = map(int, B.shape)
-            if naux != self.naux or tuple(barL.shape) != (naux, ntri):
-                raise ValueError("packed-Qp B_ao and bar_L_ao must both have shape (naux, ntri)")
-            nao = _nao_from_ntri(ntri)
-            if nao != self.nao:
-                raise ValueError("B_ao shape mismatch with context nao")
-            return _unpack_Qp(B, nao).permute(1, 2, 0).contiguous(), _unpack_Qp(barL, nao).contiguous()
+    def _mnQ_and_bar(self, B: torch.Tensor, barL: torch.Tensor):
         if B.ndim != 3 or B.shape[0] != B.shape[1]:
             raise ValueError("B_ao must have shape (nao, nao, naux)")
         if tuple(B.shape) != (self.nao, self.nao, self.naux):
@@ -94,19 +78,54 @@ class DFGradContractionContext:
             raise ValueError("bar_L_ao must have shape (naux, nao, nao)")
         return B.contiguous(), barL.contiguous()
 
-    def _contract_adjoints(self, bar_X: torch.Tensor, bar_V: torch.Tensor) -> torch.Tensor:
+    def _contract_adjoints(self, bar_X: torch.Tensor, bar_V: torch.Tensor, precision: str = "fp64") -> torch.Tensor:
         grad = torch.zeros((self.natm, 3), dtype=torch.float64, device=self.engine.device)
-        self.engine.deriv3c(bar_X, grad, layout="Qmn")
-        self.engine.deriv2c(bar_V, grad)
+        self.engine.deriv3c(bar_X, grad, layout="Qmn", precision=precision)
+        self.engine.deriv2c(bar_V, grad, precision=precision)
+        return grad
+
+    def _contract_packed(self, B_Qp: torch.Tensor, barL_Qp: torch.Tensor, aux_block_naux: int,
+                         precision: str = "fp64") -> torch.Tensor:
+        """Packed-Qp route: adjoints in packed form, then the derivative integrals one aux-shell
+        block at a time with that block's adjoint unpacked (one (q, nao, nao) block alive)."""
+        nao = self.nao
+        bar_X, bar_V = whitened_adjoints_qp(B_Qp, barL_Qp, self.L_metric, nao)
+        eng = self.engine
+        dev = eng.device
+        grad = torch.zeros((self.natm, 3), dtype=torch.float64, device=dev)
+        i, j = torch.tril_indices(nao, nao, device=dev)
+        blocks = eng.aux_blocks(max(1, int(aux_block_naux)))
+        qmax = max(p1 - p0 for p0, p1, _ in blocks)
+        buf = torch.empty((qmax, nao, nao), dtype=torch.float64, device=dev)
+        self.last_peak_block_elems = int(buf.numel())
+        for p0, p1, blk in blocks:
+            G = buf[: p1 - p0]
+            G[:, i, j] = bar_X[p0:p1]
+            G[:, j, i] = bar_X[p0:p1]
+            eng.deriv3c_block(blk, G, grad, precision=precision)
+        eng.deriv2c(bar_V, grad, precision=precision)
         return grad
 
     # ------------------------------------------------------------ contractions
-    def contract_device(self, *, B_ao: Any, bar_L_ao: Any) -> torch.Tensor:
-        B, barL = self._mnQ_and_bar(B_ao, bar_L_ao)
-        return self._contract_adjoints(*whitened_adjoints(B, barL, self.L_metric))
+    def contract_device(self, *, B_ao: Any, bar_L_ao: Any, aux_block_naux: int = 128,
+                        precision: str = "fp64") -> torch.Tensor:
+        """(natm, 3) device gradient; ``precision='mixed'`` runs the derivative integrals with FP32
+        recurrences and accumulators (``DFB_PREC_MIXED``); the adjoints stay FP64."""
+        dev = self.engine.device
+        B = torch.as_tensor(B_ao, dtype=torch.float64, device=dev)
+        barL = torch.as_tensor(bar_L_ao, dtype=torch.float64, device=dev)
+        if B.ndim == 2 and barL.ndim == 2:
+            naux, ntri = map(int, B.shape)
+            if naux != self.naux or tuple(barL.shape) != (naux, ntri):
+                raise ValueError("packed-Qp B_ao and bar_L_ao must both have shape (naux, ntri)")
+            if _nao_from_ntri(ntri) != self.nao:
+                raise ValueError("B_ao shape mismatch with context nao")
+            return self._contract_packed(B.contiguous(), barL.contiguous(), aux_block_naux, precision)
+        B, barL = self._mnQ_and_bar(B, barL)
+        return self._contract_adjoints(*whitened_adjoints(B, barL, self.L_metric), precision=precision)
 
-    def contract(self, *, B_ao: Any, bar_L_ao: Any) -> np.ndarray:
-        return self.contract_device(B_ao=B_ao, bar_L_ao=bar_L_ao).cpu().numpy()
+    def contract(self, *, B_ao: Any, bar_L_ao: Any, aux_block_naux: int = 128) -> np.ndarray:
+        return self.contract_device(B_ao=B_ao, bar_L_ao=bar_L_ao, aux_block_naux=aux_block_naux).cpu().numpy()
 
     def contract_device_fused_terms(self, *, B_ao: Any, bar_L_terms: Iterable[Any], precision: str = "fp64"):
         total = None
@@ -115,7 +134,7 @@ class DFGradContractionContext:
             total = tt.clone() if total is None else total.add_(tt)
         if total is None:
             return torch.zeros((self.natm, 3), dtype=torch.float64, device=self.engine.device)
-        return self.contract_device(B_ao=B_ao, bar_L_ao=total)
+        return self.contract_device(B_ao=B_ao, bar_L_ao=total, precision=precision)
 
     def contract_fused_terms(self, *, B_ao: Any, bar_L_terms: Iterable[Any], precision: str = "fp64") -> np.ndarray:
         return self.contract_device_fused_terms(B_ao=B_ao, bar_L_terms=bar_L_terms, precision=precision).cpu().numpy()

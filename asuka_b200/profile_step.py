@@ -59,15 +59,15 @@ def phases(eng: DFEngine, Cw: torch.Tensor, R: torch.Tensor, precision: str, X: 
     mark("metric")
     L = cholesky_metric(V)
     mark("cholesky")
-    eng.int3c("Qmn", out=X)
+    eng.int3c("Qmn", out=X, precision=precision)
     mark("int3c")
     E, J, K, saved = df_contract(eng, Cw, X, L, precision, mark)
-    G3, G2 = df_adjoints(eng, Cw, saved)
+    G3, G2 = df_adjoints(eng, Cw, saved, precision)
     mark("adjoints")
     grad = torch.zeros((eng.natm, 3), dtype=torch.float64, device="cuda")
-    eng.deriv3c(G3, grad)
+    eng.deriv3c(G3, grad, precision=precision)
     mark("deriv3c")
-    eng.deriv2c(G2, grad)
+    eng.deriv2c(G2, grad, precision=precision)
     mark("deriv2c")
     torch.cuda.synchronize()
     keys = list(ev)
@@ -76,13 +76,15 @@ def phases(eng: DFEngine, Cw: torch.Tensor, R: torch.Tensor, precision: str, X: 
     return out
 
 
-def class_times(eng, mol, top: int = 20) -> dict:
+def class_times(eng, mol, top: int = 20, precision: str = "fp64") -> dict:
     """Per-class device time of the 3c integrals and the 3c derivative contraction."""
     import ctypes
     import os
     import sys
 
     from . import _lib
+
+    pc = 0 if precision == "fp64" else 1  # DFB_PREC_FP64 / DFB_PREC_MIXED for every class
 
     sys.path.insert(0, os.path.join(os.path.dirname(os.path.abspath(__file__)), "csrc"))
     import gen_classes
@@ -99,8 +101,9 @@ def class_times(eng, mol, top: int = 20) -> dict:
         res = []
         for la, lb, lc, pairs, auxs in eng.classes3c:
             args = [la, lb, lc, ctypes.byref(eng.ps_ao), ctypes.byref(eng.axs), _lib.ptr(pairs), _lib.ptr(auxs),
-                    pairs.numel() * auxs.numel(), auxs.numel(), 0, _lib.ptr(X), nao * nao, nao, 1]
-            fn = L.dfb_rys_deriv if deriv else L.dfb_rys_int
+                    pairs.numel() * auxs.numel(), -pairs.numel(), 0, pc, _lib.ptr(X), nao * nao,
+                    nao, 1]
+            fn = L.dfb_rys_deriv_prec if deriv else L.dfb_rys_int_prec
             if deriv:
                 args += [_lib.ptr(g), eng.natm]
             args += [_lib.ptr(scr), scr.numel(), st]
@@ -111,7 +114,8 @@ def class_times(eng, mol, top: int = 20) -> dict:
                 _lib.check(fn(*args), "class timing")
             e1.record()
             torch.cuda.synchronize()
-            plan = gen_classes.plan(la, lb, lc, deriv) if la <= gen_classes.LA_MAX and lc <= gen_classes.LC_MAX else None
+            plan = (gen_classes.plan(la, lb, lc, deriv, f32=precision != "fp64")
+                    if la <= gen_classes.LA_MAX and lc <= gen_classes.LC_MAX else None)
             res.append((e0.elapsed_time(e1) / 3, f"({la},{lb},{lc})", pairs.numel() * auxs.numel(),
                         "warp" if plan is None else f"thread FS={plan[0]}{' split' if plan[1] else ''}"))
         res.sort(reverse=True)
@@ -126,7 +130,7 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--workload", default="w8", choices=sorted(WORKLOADS))
     ap.add_argument("--steps", type=int, default=3)
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed"])
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "mixed", "mixed_all"])
     ap.add_argument("--only", default=None, choices=[None, "int3c", "deriv3c", "metric", "deriv2c", "step"])
     ap.add_argument("--classes", action="store_true", help="time every angular class of int3c and deriv3c")
     ap.add_argument("--cls", default=None, metavar="LA,LB,LC",
@@ -152,7 +156,7 @@ def main():
                               **{k: (round(v, 3) if isinstance(v, float) else v) for k, v in st.items()}}))
         return
     if args.classes:
-        print(json.dumps(class_times(eng, mol)))
+        print(json.dumps(class_times(eng, mol, precision=args.precision)))
         return
     X = torch.empty((eng.naux, eng.nao, eng.nao), dtype=torch.float64, device="cuda")
     if args.only in ("int3c", "deriv3c", "metric", "deriv2c"):
@@ -162,13 +166,13 @@ def main():
             X.fill_(1e-3)
         for _ in range(args.steps):
             if args.only == "int3c":
-                eng.int3c("Qmn", out=X)
+                eng.int3c("Qmn", out=X, precision=args.precision)
             elif args.only == "metric":
                 eng.metric()
             elif args.only == "deriv3c":
-                eng.deriv3c(X, g)
+                eng.deriv3c(X, g, precision=args.precision)
             else:
-                eng.deriv2c(bar2, g)
+                eng.deriv2c(bar2, g, precision=args.precision)
         torch.cuda.synchronize()
         print(json.dumps({"only": args.only, "steps": args.steps}))
         return

@@ -10,6 +10,10 @@ density for J (UHF alpha/beta), with the same argument meaning.  Per call:
 * d = V^-1 rho, W_j = L^-1 Y_j (block substitution), K_j = sum_Q W_jQ W_jQ^T;
 * pass 2: J = sum_P d_P X_P with the blocks recomputed.
 
+``precision='mixed'`` evaluates the integrals with FP32 recurrence tables and
+accumulators (``DFB_PREC_MIXED``) and the exchange update as a split-BF16
+tensor-core GEMM; the SCF finishes with FP64 iterations.
+
 Outputs are symmetric FP64 device tensors.
 """
 
@@ -21,7 +25,7 @@ from typing import Any
 import torch
 
 from . import linalg as _la
-from . import mixed as _mixed
+from . import tc as _tc
 from .df import DFEngine, cholesky_metric, get_engine
 
 
@@ -83,7 +87,7 @@ def df_JKs_streamed(ctx: StreamedDFJKContext, D, C_occ_list: list, occ_vals_list
     Xbuf = torch.zeros((bmax, nao, nao), dtype=torch.float64, device=dev)
     Df = D.reshape(-1)
     for p0, p1, blk in ctx.aux_blocks:
-        Xb = eng.int3c_block(blk, p0, p1, out=Xbuf[: p1 - p0], dropped_zero=True)
+        Xb = eng.int3c_block(blk, p0, p1, out=Xbuf[: p1 - p0], dropped_zero=True, precision=precision)
         torch.mv(Xb.view(p1 - p0, -1), Df, out=rho[p0:p1])
         for Cw, Y, n in zip(Cws, Ys, noccs):
             if n:
@@ -98,11 +102,11 @@ def df_JKs_streamed(ctx: StreamedDFJKContext, D, C_occ_list: list, occ_vals_list
             _la.solve_lower(L, Y, ctx.L_inv_blocks, out=Y)
             W3 = Y.view(naux, nao, n)
             for q0 in range(0, naux, qb):
-                Wc = W3[q0:q0 + qb].permute(1, 0, 2).reshape(nao, -1)
-                if precision == "fp64" or nao < _mixed.MIN_DIM:
+                if precision == "fp64":
+                    Wc = W3[q0:q0 + qb].permute(1, 0, 2).reshape(nao, -1)
                     K.addmm_(Wc, Wc.T)
                 else:
-                    K += _mixed.syrk(Wc)
+                    _tc.syrk_qblocks(W3[q0:q0 + qb], out=K)
         Ks.append(0.5 * (K + K.T))
     del Ys
     J = torch.zeros((nao, nao), dtype=torch.float64, device=dev)
@@ -111,7 +115,7 @@ def df_JKs_streamed(ctx: StreamedDFJKContext, D, C_occ_list: list, occ_vals_list
         if len(ctx.aux_blocks) == 1:
             Xb = Xbuf[: p1 - p0]  # still holds the only block
         else:
-            Xb = eng.int3c_block(blk, p0, p1, out=Xbuf[: p1 - p0], dropped_zero=True)
+            Xb = eng.int3c_block(blk, p0, p1, out=Xbuf[: p1 - p0], dropped_zero=True, precision=precision)
         Jf.addmv_(Xb.view(p1 - p0, -1).T, d[p0:p1])
     return 0.5 * (J + J.T), Ks
 

@@ -13,8 +13,8 @@ contracted on the fly).  ``value`` times it with inputs resident on the GPU;
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
 
-With N > 1 (torchrun) every rank runs an independent replica of the step
-(the north-star path is single-GPU; see DESIGN.md "replicas only").
+With N > 1 (torchrun) every rank runs an independent replica of the step: the
+path runs on one GPU, so there is no exchange between ranks.
 """
 
 from __future__ import annotations

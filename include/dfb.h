@@ -22,32 +22,7 @@
 extern "C" {
 #endif
 
-#define DFB_OK 0
-#define DFB_ERR_INVALID (-1)
-#define DFB_ERR_CUDA (-2)
-#define DFB_ERR_UNSUPPORTED (-3)
-#define DFB_ERR_NOT_INITIALISED (-4)
-
-/* AB side of a Rys task: AO shell pairs (A,B), or aux self-pairs (P, dummy). */
-typedef struct {
-    const int *shA, *shB;          /* per pair: shell indices in the AB basis (shB unused if b_dummy) */
-    const int *pstart, *npair;     /* per pair: primitive-pair range in the tables below */
-    const double *eta, *Px, *Py, *Pz, *cK;  /* per primitive pair */
-    const double *ea, *eb;         /* per primitive pair: exponents of the A and B primitives */
-    const double *cxyz;            /* AB basis shell centres (nshell, 3) */
-    const int *aostart;            /* AB basis first function of each shell */
-    const int *atom;               /* AB basis shell -> atom */
-    int b_dummy;                   /* 1: B is the dummy s shell (metric) */
-} dfb_pair_side_t;
-
-/* C side of a Rys task: one aux shell (the dummy D is implicit). */
-typedef struct {
-    const double *cxyz;
-    const int *pstart, *nprim;
-    const double *pexp, *pcoef;
-    const int *aostart;
-    const int *atom;
-} dfb_aux_side_t;
+#include "dfb_types.h"
 
 /* Library version (major*10000+minor*100+patch). */
 int dfb_version(void);
@@ -118,15 +93,25 @@ int dfb_rys_deriv(int la, int lb, int lc, const dfb_pair_side_t *ps, const dfb_a
  */
 int dfb_fp64_fma_probe(double *out, int blocks, int threads, int iters, void *stream);
 
+/* FP32 FMA throughput probe (the roofline denominator of the FP32 recurrences of the
+ * mixed-precision Rys kernels): blocks x threads threads each run iters x 64 FMAs in
+ * 16 independent chains; out holds blocks*threads floats.  No reference counterpart. */
+int dfb_fp32_fma_probe(float *out, int blocks, int threads, int iters, void *stream);
+
+/* Number of kernels the library has launched in this process (all entry points). */
+long dfb_launch_count(void);
+
 /*
  * Allocation-free variant of dfb_rys_int for callers that cannot allocate
  * device memory (frameworks that hand over only input/output buffers, code
  * under an allocator that forbids new device allocations).  No counterpart in
  * the reference.  Same arguments and output as dfb_rys_int without the
- * scratch buffer: the generic warp kernel uses a fixed 8 MiB scratch array in
- * the library's device image (held by every GPU that loads the library), the
- * persistent grid is shrunk to fit it, and classes that need more than it holds
- * per block fail with DFB_ERR_UNSUPPORTED.  The first call on a device looks up
+ * scratch buffer: the generic warp kernel uses a fixed 8 MiB scratch array
+ * (2^20 doubles) in the library's device image (held by every GPU that loads the
+ * library), and the class's tasks run in batches of floor(2^20 / slot) tasks per
+ * pair of launches, slot being one task's contracted intermediate; a class fails
+ * with DFB_ERR_UNSUPPORTED only if a single task's slot exceeds the array (none
+ * with l <= 8 does).  The first call on a device looks up
  * the array's address and should come before any stream capture; calls share
  * the array, so calls that overlap on the GPU race.  dfb_rys_table_init must
  * have run on the device.
@@ -134,6 +119,58 @@ int dfb_fp64_fma_probe(double *out, int blocks, int threads, int iters, void *st
 int dfb_rys_int_noalloc(int la, int lb, int lc, const dfb_pair_side_t *ps, const dfb_aux_side_t *aux,
                         const int *task_pair, const int *task_aux, long ntask, long naux_grid, int mode, double *out,
                         long sP, long sM, long sN, void *stream);
+
+/* Precision of the Rys kernels (dfb_rys_int_prec, dfb_rys_deriv_prec). */
+#define DFB_PREC_FP64 0  /* every step in FP64 (the reference's arithmetic) */
+#define DFB_PREC_MIXED 1 /* FP64 roots, weights, prefactors, horizontal recurrence, adjoint contraction and
+                            gradient accumulation; FP32 2D recurrence tables and per-task accumulation */
+
+/*
+ * dfb_rys_int / dfb_rys_deriv with a precision argument.  DFB_PREC_MIXED runs
+ * the class-specialised kernels with FP32 recurrence tables and accumulators
+ * (about 1e-7 relative per integral); classes that have no specialised
+ * kernel run in FP64 either way.  The reference's counterpart is its
+ * mixed-precision Rys tile kernels (kMixedPrec,
+ * asuka/cueri/cuda/ext/src/generated/cueri_cuda_kernels_wave1_generated.cu:1536)
+ * switched on by CuERIDFConfig.mixed_precision (asuka/integrals/cueri_df.py:61-65).
+ */
+int dfb_rys_int_prec(int la, int lb, int lc, const dfb_pair_side_t *ps, const dfb_aux_side_t *aux,
+                     const int *task_pair, const int *task_aux, long ntask, long naux_grid, int mode, int precision,
+                     double *out, long sP, long sM, long sN, double *scratch, long scratch_doubles, void *stream);
+int dfb_rys_deriv_prec(int la, int lb, int lc, const dfb_pair_side_t *ps, const dfb_aux_side_t *aux,
+                       const int *task_pair, const int *task_aux, long ntask, long naux_grid, int mode, int precision,
+                       const double *bar, long sbP, long sbM, long sbN, double *grad, int natm, double *scratch,
+                       long scratch_doubles, void *stream);
+
+/*
+ * One operand of dfb_tc_gemm.  Element (row, k) of batch entry b is
+ *   ptr[b*s_batch + row*s_row + (k / nk1)*s_kq + (k % nk1)*s_k1],
+ * so strided views need no copy (the exchange update's W[Q, mu, i] with k = (Q, i):
+ * s_row = nocc, s_kq = nao*nocc, s_k1 = 1, nk1 = nocc).
+ */
+typedef struct {
+    const double *ptr;
+    long s_row, s_kq, s_k1, nk1, s_batch;
+} dfb_tc_operand_t;
+
+/*
+ * Split-BF16 tensor-core GEMM (tcgen05, sm_100a):
+ *   C[b][m*ldc + n] (+)= sum_k A(m, k) B(n, k),  b < batch, C at C + b*s_cbatch.
+ * Each FP64 element is split into nterms (2 or 3) bfloat16 terms; the products of
+ * order <= 2^-8 (nterms 2) or 2^-16 (nterms 3) run on the tensor cores with FP32
+ * accumulation over k spans of kspan (<= 0: all of K), and the spans are combined
+ * in FP64.  accumulate=0 stores C (needs one span, kspan >= K); accumulate=1 adds
+ * with FP64 atomics (C must hold the start value).  symmetric=1 (A == B, M == N)
+ * computes the tiles on and above the diagonal and mirrors them.  About 1e-7
+ * relative (nterms 3).  Replaces the reference's cuBLAS DGEMM calls of the DF J/K
+ * workspace (asuka/hf/cuda/ext/src/hf_df_jk_cuda_ext.cpp:231-598) in mixed mode.
+ */
+int dfb_tc_gemm(long M, long N, long K, long batch, const dfb_tc_operand_t *A, const dfb_tc_operand_t *B, double *C,
+                long ldc, long s_cbatch, int accumulate, int symmetric, int nterms, long kspan, void *stream);
+
+/* First error code recorded by a bounded wait inside the tensor-core kernels since the
+ * last reset (0 = none; 1, 2 = an mbarrier wait gave up).  Synchronous. */
+int dfb_tc_error(int reset);
 
 /* Scratch doubles dfb_rys_int / dfb_rys_deriv need for this class and task count. */
 long dfb_rys_scratch_doubles(int la, int lb, int lc, long ntask, int deriv);

@@ -108,6 +108,111 @@ def scf_case(name: str, mol, with_grad: bool = True) -> None:
     print(f"{name}: nao={nao} naux={naux} E={res.e_tot:.12f} iters={res.scf.niter} t_scf={t_scf:.1f}s", flush=True)
 
 
+def scf_grad_small_case(name: str, mol, with_grad: bool = True) -> None:
+    """Like ``scf_case`` for systems whose 3c tensor is too large for a fixture.
+
+    Keeps only what the parity tests compare: the converged energy, the orbital
+    energies, the weighted occupied orbitals Cw = C_occ sqrt(occ) (the density at
+    which the two-electron energy and gradient are evaluated), E_2e at that
+    density, and the reference's DF two-electron gradient there.
+    """
+    from asuka.frontend.scf import run_hf_df
+    from asuka.integrals.grad import compute_df_gradient_contributions_analytic_packed_bases
+
+    rmol = _ref_mol(mol)
+    t0 = time.perf_counter()
+    res = run_hf_df(rmol, method="rhf", backend="cpu", df=True, auxbasis="ricd", conv_tol=1e-10)
+    t_scf = time.perf_counter() - t0
+    B = np.asarray(res.df_B)
+    L = np.asarray(res.df_L)
+    nao, _, naux = B.shape
+    C = np.asarray(res.mo_coeff)
+    occ = np.asarray(res.mo_occ)
+    nocc = int((occ > 0).sum())
+    Cw = C[:, :nocc] * np.sqrt(occ[:nocc])[None, :]
+    D = Cw @ Cw.T
+    rho = np.tensordot(D, B, axes=([0, 1], [0, 1]))
+    # E_2e = 1/2 rho.rho - 1/4 sum_Q |Cw^T B_Q Cw|^2 (the DF Coulomb and exchange energies at D)
+    M = np.tensordot(np.tensordot(Cw, B, axes=(0, 0)), Cw, axes=(1, 0))  # (i, Q, j)
+    E2 = 0.5 * float(rho @ rho) - 0.25 * float(np.sum(M * M))
+    del M
+    out = dict(elements=np.array(mol.elements), coords_bohr=mol.coords_bohr, basis=np.array(mol.basis),
+               nao=np.array(nao), naux=np.array(naux), e_nuc=np.array(res.e_nuc), e_tot=np.array(res.e_tot),
+               niter=np.array(res.scf.niter), mo_energy=np.asarray(res.mo_energy), Cw=Cw, E2=np.array(E2),
+               t_scf_s=np.array(t_scf), threads=np.array(int(os.environ.get("OMP_NUM_THREADS", "0"))))
+    if with_grad:
+        # bar_L[Q] = dE_2e/dB_Q = rho_Q D - 1/2 D B_Q D
+        DBD = np.tensordot(np.tensordot(D, B, axes=(1, 0)), D, axes=(1, 0))  # (m, Q, l)
+        barL = np.ascontiguousarray(DBD.transpose(1, 0, 2))
+        del DBD
+        barL *= -0.5
+        barL += rho[:, None, None] * D[None, :, :]
+        t0 = time.perf_counter()
+        g2 = compute_df_gradient_contributions_analytic_packed_bases(
+            res.ao_basis, res.aux_basis, atom_coords_bohr=mol.coords_bohr, B_ao=B, bar_L_ao=barL, L_chol=L,
+            backend="cpu")
+        out["grad_2e"] = np.asarray(g2)
+        out["t_grad_s"] = np.array(time.perf_counter() - t0)
+    np.savez_compressed(os.path.join(HERE, f"{name}.npz"), **out)
+    print(f"{name}: nao={nao} naux={naux} E={res.e_tot:.12f} iters={res.scf.niter} t_scf={t_scf:.1f}s", flush=True)
+
+
+def int1e_grad_case(name: str, mol) -> None:
+    """The reference's one-electron gradient contractions (``asuka/integrals/int1e_cart.py:1452,1738``)
+    with a seeded random symmetric M, and its nuclear-repulsion gradient (``molecule.py:148``)."""
+    from asuka.frontend.one_electron import build_ao_basis_cart
+    from asuka.integrals.int1e_cart import contract_dhcore_cart, contract_dS_cart
+
+    rmol = _ref_mol(mol)
+    ao, _ = build_ao_basis_cart(rmol, basis=mol.basis, expand_contractions=True)
+    nao = int(np.asarray(ao.shell_ao_start)[-1] + (np.asarray(ao.shell_l)[-1] + 1) * (np.asarray(ao.shell_l)[-1] + 2) // 2)
+    rng = np.random.default_rng(7)
+    M = rng.standard_normal((nao, nao))
+    M = 0.5 * (M + M.T)
+    Z = np.array([float(z) for z in rmol.atom_charges()]) if hasattr(rmol, "atom_charges") else None
+    if Z is None:
+        from asuka.frontend.molecule import atomic_number
+
+        Z = np.array([float(atomic_number(a)) for a, _ in rmol.atoms_bohr])
+    R = np.asarray(mol.coords_bohr)
+    gS = contract_dS_cart(ao, atom_coords_bohr=R, M=M, contract_backend="cpu")
+    gH = contract_dhcore_cart(ao, atom_coords_bohr=R, atom_charges=Z, M=M, contract_backend="cpu")
+    gH0 = contract_dhcore_cart(ao, atom_coords_bohr=R, atom_charges=Z, M=M, include_operator_deriv=False,
+                               contract_backend="cpu")
+    np.savez_compressed(os.path.join(HERE, f"{name}.npz"), elements=np.array(mol.elements), coords_bohr=R,
+                        basis=np.array(mol.basis), M=M, Z=Z, gS=np.asarray(gS), gH=np.asarray(gH),
+                        gH_basis_only=np.asarray(gH0), g_nuc=np.asarray(rmol.energy_nuc_grad()))
+    print(f"{name}: nao={nao}", flush=True)
+
+
+def casscf_barl_case(name: str) -> None:
+    """The reference's CASSCF DF-gradient adjoint builders (``asuka/mcscf/nuc_grad_df.py:2387-2600``,
+    ``_build_bar_L_casscf_df`` for B in mnQ and in packed Qp) on seeded inputs: a symmetric B
+    (nao, nao, naux), core and active densities, active orbitals and a symmetric 2-RDM."""
+    from asuka.integrals.df_packed_s2 import pack_B_to_Qp
+    from asuka.mcscf.nuc_grad_df import _build_bar_L_casscf_df
+
+    rng = np.random.default_rng(11)
+    nao, naux, ncore, ncas = 24, 61, 3, 4
+    B = rng.standard_normal((nao, nao, naux))
+    B = 0.5 * (B + B.transpose(1, 0, 2))
+    C = np.linalg.qr(rng.standard_normal((nao, ncore + ncas)))[0]
+    D_core = 2.0 * C[:, :ncore] @ C[:, :ncore].T
+    C_act = np.ascontiguousarray(C[:, ncore:])
+    g1 = rng.standard_normal((ncas, ncas))
+    dm1 = g1 @ g1.T
+    D_act = C_act @ dm1 @ C_act.T
+    t = rng.standard_normal((ncas * ncas, ncas * ncas))
+    dm2 = (t + t.T).reshape(ncas, ncas, ncas, ncas)
+    dm2 = 0.5 * (dm2 + dm2.transpose(1, 0, 3, 2))  # (uv|xy) = (vu|yx)
+    bar = _build_bar_L_casscf_df(B, D_core_ao=D_core, D_act_ao=D_act, C_act=C_act, dm2_act=dm2)
+    BQp = np.asarray(pack_B_to_Qp(B, layout="mnQ", nao=nao))
+    bar_qp = _build_bar_L_casscf_df(BQp, D_core_ao=D_core, D_act_ao=D_act, C_act=C_act, dm2_act=dm2)
+    np.savez_compressed(os.path.join(HERE, f"{name}.npz"), B=B, D_core=D_core, D_act=D_act, C_act=C_act, dm2=dm2,
+                        bar=np.asarray(bar), B_Qp=BQp, bar_qp=np.asarray(bar_qp))
+    print(f"{name}: bar {np.asarray(bar).shape}, bar_qp {np.asarray(bar_qp).shape}", flush=True)
+
+
 def tiles_case(name: str, mol) -> None:
     """One (ab|P) tile per (la, lb, lP) class and one (P|Q) tile per (lP, lQ) class."""
     from asuka.cueri import _eri_rys_cpu as ext
@@ -213,6 +318,12 @@ CASES = {
     "h2o_masvp": lambda: scf_case("h2o_masvp", geo.water("ma-svp")),
     "h2o_matzvp": lambda: scf_case("h2o_matzvp", geo.water("ma-tzvp")),
     "tiles_h2o_maqzvp": lambda: tiles_case("tiles_h2o_maqzvp", geo.water("ma-qzvp")),
+    # the three larger workloads: (H2O)8 seed 0 / ma-TZVP, all-trans n-decane seed 0 / ma-SVP, H2O / ma-QZVP
+    "int1e_grad_h2o_matzvp": lambda: int1e_grad_case("int1e_grad_h2o_matzvp", geo.water("ma-tzvp")),
+    "casscf_barl": lambda: casscf_barl_case("casscf_barl"),
+    "w8_matzvp": lambda: scf_grad_small_case("w8_matzvp", geo.water_cluster(8, 0, "ma-tzvp")),
+    "decane_masvp": lambda: scf_grad_small_case("decane_masvp", geo.decane(0, "ma-svp")),
+    "h2o_maqzvp": lambda: scf_grad_small_case("h2o_maqzvp", geo.water("ma-qzvp")),
     "ref_roots": roots_case,
     "cart2sph_ref": sph_case,
     "sph_h2o_matzvp": lambda: sph_scf_case("sph_h2o_matzvp", geo.water("ma-tzvp")),

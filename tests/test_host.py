@@ -140,3 +140,41 @@ def test_class_planner_budget_and_table(tmp_path, monkeypatch):
     monkeypatch.setenv("DFB_GEN_NO_TUNING", "1")
     assert gc.tuning() == {}
     assert gc.plan(1, 0, 4, True) == gc.plan(1, 0, 4, True, budget=66)
+
+
+def test_overlap_gradient_contraction_matches_reference():
+    """sum M . dS/dR against the reference's contract_dS_cart (int1e_cart.py:1452), H2O / ma-TZVP."""
+    from asuka_b200.geometry import Molecule
+    from asuka_b200.int1e import contract_dS_cart
+
+    g = golden("int1e_grad_h2o_matzvp")
+    ao, _aux, _sp = bases_of(g)
+    gS = contract_dS_cart(ao, atom_coords_bohr=g["coords_bohr"], M=g["M"])
+    assert np.abs(gS - g["gS"]).max() < 1e-12 * np.abs(g["gS"]).max()
+    mol = Molecule.from_atoms([(str(e), x) for e, x in zip(g["elements"], g["coords_bohr"])], unit="Bohr",
+                              basis=str(g["basis"]))
+    assert np.abs(mol.energy_nuc_grad() - g["g_nuc"]).max() < 1e-13
+
+
+def test_kinetic_gradient_contraction_matches_finite_differences():
+    """sum M . dT/dR (and dS/dR) against central differences of the host T and S builds."""
+    from asuka_b200 import basis as bm
+    from asuka_b200.int1e import build_S_T, contract_dS_T_cart
+
+    g = golden("int1e_grad_h2o_matzvp")
+    ao, _aux, _sp = bases_of(g)
+    M = g["M"]
+    gS, gT = contract_dS_T_cart(ao, M, M, np.asarray(ao.shell_atom), 3)
+    R0 = g["coords_bohr"]
+    h = 1e-5
+    for (a, c) in [(0, 0), (1, 1), (2, 2)]:
+        vals = []
+        for s in (1, -1):
+            R = R0.copy()
+            R[a, c] += s * h
+            b = bm.pack_basis([(str(e), x) for e, x in zip(g["elements"], R)], str(g["basis"]), "ao")
+            vals.append(build_S_T(b))
+        fdS = float(((vals[0][0] - vals[1][0]) * M).sum() / (2 * h))
+        fdT = float(((vals[0][1] - vals[1][1]) * M).sum() / (2 * h))
+        assert abs(fdS - gS[a, c]) < 1e-8 * max(1.0, abs(fdS))
+        assert abs(fdT - gT[a, c]) < 1e-8 * max(1.0, abs(fdT))
