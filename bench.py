@@ -53,10 +53,19 @@ def _workload():
     return mol, bm.pack_basis(atoms, "ma-tzvp", "ao"), bm.pack_basis(atoms, "ma-tzvp", "aux")
 
 
-# DRAM bytes (read + write) of one 3c derivative contraction of this workload (all class launches of
-# one gradient), from one ncu capture: --metrics dram__bytes_read.sum,dram__bytes_write.sum -k regex:k_rys
-# on `python -m asuka_b200.profile_step --workload w8 --only deriv3c --steps 1` (3.467e9 + 0.025e9).
-DERIV3C_DRAM_BYTES = 3.492e9
+TRAFFIC_FILE = os.path.join(ROOT, "profiles", "dram_traffic_deriv3c_h2o8_matzvp.txt")
+
+
+def _deriv3c_traffic():
+    """DRAM bytes (read + write) of one 3c derivative contraction of this workload (all class launches
+    of one gradient) and the capture they come from, read from the committed ncu summary."""
+    if not os.path.exists(TRAFFIC_FILE):
+        return None, None
+    with open(TRAFFIC_FILE) as f:
+        for line in f:
+            if line.startswith("bytes_per_launch_set:"):
+                return float(line.split(":", 1)[1].split()[0]), os.path.relpath(TRAFFIC_FILE, ROOT)
+    return None, None
 
 
 def flops_3c(ao, aux, deriv: bool = False) -> float:
@@ -213,9 +222,10 @@ def run_reference(args) -> dict:
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": WORKLOAD, "precision": "fp64 (reference CPU)"},
             "cpu_baseline": {"value": ms, "unit": "ms", "cores": cores, "kind": "reference",
-                             "sample": f"3c and 3c-derivative loops over every {stride}th AO shell pair "
-                                       f"({100 * frac:.2f}% of primitive-pair work), scaled; metric, Cholesky, "
-                                       f"whitening, J/K, adjoints, 2c derivatives at full size"},
+                             "sample": f"3c and 3c-derivative loops over every {stride}th AO shell pair of each "
+                                       f"(la, lb) class ({100 * frac:.2f}% of primitive-pair work), each class "
+                                       f"scaled by its sampled work fraction; metric, Cholesky, whitening, J/K, "
+                                       f"adjoints, 2c derivatives at full size"},
             "e2e": {"value": ms, "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
             "phases_s": {k: round(v, 4) for k, v in r.items() if isinstance(v, float) and k != "E2"}}
 
@@ -261,43 +271,24 @@ def run_gpu(args) -> dict | None:
     dE_step = abs(float(E64) - float(Emx))
     dG_step = float((g64 - gmx).abs().max())
 
-    # count our kernel launches in one step
     import asuka_b200._lib as _l
-
-    calls = {"n": 0}
-    real = _l.lib()
-    orig = {n: getattr(real, n) for n in ("dfb_rys_int", "dfb_rys_deriv", "dfb_pair_tables")}
-
-    class _Count:
-        def __getattr__(self, n):
-            f = orig.get(n)
-            if f is None:
-                return getattr(real, n)
-
-            def w(*a):
-                calls["n"] += 1
-                return f(*a)
-
-            return w
-
-    _l._LIB = _Count()
-    step("mixed")
-    _l._LIB = real
-    launches_per_step = calls["n"]
 
     stream = torch.cuda.current_stream(dev)
     results = {}
+    launches = {}
     for prec in ("fp64", "mixed"):
         for _ in range(args.warmup):
             step(prec)
         _barrier(world)
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        n0 = _l.lib().dfb_launch_count()  # kernels this library launches (counted at every launch site)
         with ClockSampler() as cs:
             e0.record(stream)
             for _ in range(args.steps):
                 step(prec)
             e1.record(stream)
             _barrier(world)
+        launches[prec] = int(_l.lib().dfb_launch_count() - n0)
         results[prec] = (_reduce_max(e0.elapsed_time(e1) / args.steps, world), cs.summary())
 
     # roofline of the dominant kernel family: the 3c derivative contraction (FP64 CUDA cores)
@@ -316,9 +307,10 @@ def run_gpu(args) -> dict | None:
     torch.cuda.synchronize()
     t_d3 = e0.elapsed_time(e1) / nrep
     fl = flops_deriv3c(ao, aux)
-    from asuka_b200.peaks import fp64_dgemm_tflops, fp64_fma_tflops
+    from asuka_b200.peaks import fp32_fma_tflops, fp64_dgemm_tflops, fp64_fma_tflops
 
     fp64_peak = fp64_fma_tflops(dev)
+    fp32_peak = fp32_fma_tflops(dev)
     fp64_src = "measured live: FP64 FMA probe (dfb_fp64_fma_probe), all SMs, best of 5"
     dgemm_peak = fp64_dgemm_tflops(4096, dev)
     achieved = fl / (t_d3 * 1e-3) / 1e12
@@ -395,16 +387,21 @@ def run_gpu(args) -> dict | None:
     if rank != 0:
         return None
 
+    traffic, traffic_src = _deriv3c_traffic()
+    tab = dfmod.mixed_class_table()
+    mixed_counts = ", ".join(f"{len(tab.get(k, ()))} {k}" for k in ("int3c", "deriv3c", "deriv2c"))
     ms_mx, clk = results["mixed"]
     ms_64, clk64 = results["fp64"]
     out = {
         "metric": METRIC, "value": round(ms_mx, 4), "unit": "ms", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(ms_mx, 4), "higher_is_better": False, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded geometry; basis tables from the reference)",
-        "config": {"workload": WORKLOAD, "nao": nao, "naux": naux, "precision": "mixed (split-BF16 exchange update"
-                   " above its measured crossover nao >= 1024, FP64 below it and for the integrals, solves and"
-                   " gradient accumulation)", "l2": "working set (3c tensor 2.5 GB) > L2 126 MB",
-                   "replicas": world if world > 1 else None},
+        "config": {"workload": WORKLOAD, "nao": nao, "naux": naux,
+                   "precision": "mixed: FP32-component Rys kernels for the angular classes the precision table admits "
+                                f"({mixed_counts}, chosen by asuka_b200.tune_precision within 2.5e-7 Eh and 2.5e-7 "
+                                "Eh/bohr), split-BF16 tcgen05 exchange update; FP64 roots/weights, metric, solves, "
+                                "Y = X Cw, adjoints, energy and gradient accumulation",
+                   "l2": "working set (3c tensor 2.5 GB) > L2 126 MB", "replicas": world if world > 1 else None},
         "fp64_ms_per_step": round(ms_64, 4),
         "mixed_speedup_vs_fp64": round(ms_64 / ms_mx, 4),
         "accuracy": {"scf_dE_mixed_vs_fp64_Eh": abs(scfmx.e_tot - scf64.e_tot), "scf_e_tot": scf64.e_tot,
@@ -412,18 +409,19 @@ def run_gpu(args) -> dict | None:
                      "step_dE2_mixed_vs_fp64_Eh": dE_step, "step_max_dgrad_Eh_per_bohr": dG_step},
         "e2e": {"value": round(t_e2e, 4), "unit": "ms", "h2d_bytes_per_step": int(Rh.numel() * 8 + Cwh.numel() * 8),
                 "d2h_bytes_per_step": int(gh.numel() * 8 + 8)},
-        "gpu_launches": int(launches_per_step * args.steps),
+        "gpu_launches": launches["mixed"],
+        "gpu_launches_fp64_run": launches["fp64"],
         "roofline": {"kernel": "k_rys<DERIV> (3c derivative contraction, all classes)", "bound": "fp64",
                      "achieved": round(achieved, 3), "peak": fp64_peak, "unit": "TFLOP/s",
                      "frac": round(achieved / fp64_peak, 4), "peak_source": fp64_src,
                      "fp64_dgemm_tflops": round(dgemm_peak, 2),
                      "avg_launch_set_ms": round(t_d3, 4), "algorithmic_flops": fl,
-                     "traffic": DERIV3C_DRAM_BYTES, "traffic_unit": "bytes per launch set (ncu)"},
+                     "traffic": traffic, "traffic_unit": "DRAM bytes per launch set", "traffic_source": traffic_src},
         "clocks": clk, "clocks_fp64_run": clk64,
         "phases": phases_out,
         "phase_models": {"int3c_flops": f3, "deriv3c_flops": fl, "jk_dense_flops": f_jk, "adjoint_flops": f_adj,
-                         "j_bytes": j_bytes, "fp64_fma_peak_tflops": fp64_peak, "dgemm_peak_tflops": round(dgemm_peak, 2),
-                         "hbm_peak_gbs": hbm},
+                         "j_bytes": j_bytes, "fp64_fma_peak_tflops": fp64_peak, "fp32_fma_peak_tflops": fp32_peak,
+                         "dgemm_peak_tflops": round(dgemm_peak, 2), "hbm_peak_gbs": hbm},
     }
     if not args.no_cpu_baseline:
         try:
@@ -436,8 +434,8 @@ def run_gpu(args) -> dict | None:
                 r = ref_cpu.cpu_step(ao, aux, Cw.cpu().numpy(), mol.natm, pair_stride=stride)
                 out["cpu_baseline"] = {"value": round(1e3 * r["total"], 1), "unit": "ms", "cores": cores,
                                        "kind": "reference",
-                                       "sample": f"3c loops over every {stride}th AO shell pair "
-                                                 f"({100 * r['sample_fraction']:.2f}% of primitive-pair work), "
+                                       "sample": f"3c loops over every {stride}th AO shell pair of each (la, lb) "
+                                                 f"class ({100 * r['sample_fraction']:.2f}% of primitive-pair work), "
                                                  "scaled; rest at full size"}
         except Exception as exc:  # the baseline is reported, never required
             out["cpu_baseline"] = {"value": None, "error": str(exc)[:200]}

@@ -14,9 +14,13 @@ kernels (``oracle/_ref/_eri_rys_cpu*.so``, built from the reference source by
   / ``df_metric_2c2e_deriv_contracted_cart_sp_batch_cy``
   (``asuka/integrals/grad.py:420-616``).
 
-``pair_stride`` > 1 times only every stride-th AO shell pair in the two 3c
-loops (the dominant cost) and scales those loop times by the sampled fraction
-of primitive-pair work; everything else runs at full size.
+``pair_stride`` > 1 times only a sample of the AO shell pairs in the two 3c
+loops (the dominant cost): within every (la, lb) angular class every stride-th
+pair (at least one per class), each class's loop time scaled by that class's
+sampled fraction of primitive-pair work -- so the sample has the class mix of
+the whole loop.  Everything else runs at full size.  ``record`` collects the
+time of every evaluated shell pair (for checking a sampled estimate against an
+unsampled run).
 """
 
 from __future__ import annotations
@@ -73,7 +77,25 @@ def _combined(ao, aux):
                 pcoef=pcoef, spA=spA, spB=spB, npair=npair, start=start, nsp_ao=sp.nsp)
 
 
-def cpu_step(ao, aux, Cw: np.ndarray, natm: int, pair_stride: int = 1, threads: int = 0) -> dict:
+def _stratified_sample(c: dict, ao, nsp_ao: int, stride: int):
+    """Per (la, lb) class: every stride-th pair (offset stride // 2, at least one), and the class's
+    primitive-pair work in total and in the sample."""
+    la = ao.shell_l[c["spA"][:nsp_ao]]
+    lb = ao.shell_l[c["spB"][:nsp_ao]]
+    w = c["npair"][:nsp_ao].astype(np.float64)
+    out = []
+    for a in np.unique(la):
+        for b in np.unique(lb):
+            idx = np.nonzero((la == a) & (lb == b))[0]
+            if idx.size == 0:
+                continue
+            smp = idx[min(stride // 2, idx.size - 1)::max(1, stride)] if stride > 1 else idx
+            out.append((smp, float(w[idx].sum()), float(w[smp].sum())))
+    return out
+
+
+def cpu_step(ao, aux, Cw: np.ndarray, natm: int, pair_stride: int = 1, threads: int = 0,
+             record: dict | None = None) -> dict:
     """One DF J/K build + 2e nuclear gradient on the host cores; returns phase times (s, scaled)."""
     ext = load_ref()
     t = {}
@@ -109,14 +131,18 @@ def cpu_step(ao, aux, Cw: np.ndarray, natm: int, pair_stride: int = 1, threads: 
                 V[q0:q0 + nQ, p0:p0 + nP] = blk.T
     V = 0.5 * (V + V.T)
     t["metric"] = time.perf_counter() - T0
-    # 3c over sampled AO pairs
-    sample = np.arange(0, nsp_ao, max(1, int(pair_stride)))
-    w_all = float(np.sum(c["npair"][:nsp_ao]))
-    w_smp = float(np.sum(c["npair"][sample]))
-    frac = w_smp / w_all
+    # 3c over the sampled AO pairs of every angular class
+    strata = _stratified_sample(c, ao, nsp_ao, max(1, int(pair_stride)))
+    sample = np.concatenate([s for s, _, _ in strata])
+    scale = np.zeros(nsp_ao)
+    for smp, w_cls, w_smp in strata:
+        scale[smp] = w_cls / w_smp
+    frac = float(sum(ws for _, _, ws in strata) / sum(wc for _, wc, _ in strata))
     X = np.zeros((nao * nao, naux))
-    T0 = time.perf_counter()
+    t_int = 0.0
+    rec_int = record.setdefault("int3c", {}) if record is not None else None
     for sp in sample:
+        T0 = time.perf_counter()
         A, B = c["spA"][sp], c["spB"][sp]
         la, lb = ao.shell_l[A], ao.shell_l[B]
         nA, nB = (la + 1) * (la + 2) // 2, (lb + 1) * (lb + 2) // 2
@@ -131,7 +157,11 @@ def cpu_step(ao, aux, Cw: np.ndarray, natm: int, pair_stride: int = 1, threads: 
                 tile = np.asarray(tiles[k]).reshape(nA * nB, nQ)
                 X[rows, q0:q0 + nQ] = tile
                 X[rowsT, q0:q0 + nQ] = tile.reshape(nA, nB, nQ).transpose(1, 0, 2).reshape(nB * nA, nQ)
-    t["int3c"] = (time.perf_counter() - T0) / frac
+        dt = time.perf_counter() - T0
+        t_int += dt * scale[sp]
+        if rec_int is not None:
+            rec_int[int(sp)] = dt
+    t["int3c"] = t_int
     # Cholesky + whitening
     T0 = time.perf_counter()
     L = np.linalg.cholesky(V)
@@ -166,8 +196,10 @@ def cpu_step(ao, aux, Cw: np.ndarray, natm: int, pair_stride: int = 1, threads: 
     grad = np.zeros((natm, 3))
     ao_atom = ao.shell_atom
     ax_atom = aux.shell_atom
-    T0 = time.perf_counter()
+    t_der = 0.0
+    rec_der = record.setdefault("deriv3c", {}) if record is not None else None
     for sp in sample:
+        T0 = time.perf_counter()
         A, B_ = c["spA"][sp], c["spB"][sp]
         fac = 2.0 if A != B_ else 1.0
         for lq, qs in by_l.items():
@@ -179,7 +211,11 @@ def cpu_step(ao, aux, Cw: np.ndarray, natm: int, pair_stride: int = 1, threads: 
                 grad[ao_atom[A]] += fac * out[k, 0]
                 grad[ao_atom[B_]] += fac * out[k, 1]
                 grad[ax_atom[q]] += fac * out[k, 2]
-    t["deriv3c"] = (time.perf_counter() - T0) / frac
+        dt = time.perf_counter() - T0
+        t_der += dt * scale[sp]
+        if rec_der is not None:
+            rec_der[int(sp)] = dt
+    t["deriv3c"] = t_der
     T0 = time.perf_counter()
     for P in range(aux.nshell):
         for lq, qs in by_l.items():
