@@ -134,14 +134,16 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
     for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
 }
 
-// x = t0 + t1 + t2 (+ rounding below 2^-24 |x|): each term the bfloat16 rounding of what is left
+// x = t0 + t1 + t2 (+ rounding below 2^-24 |x|): each term the bfloat16 rounding of what is left.
+// The remainders are exact in FP32 (a bfloat16 term holds the leading 8 of the at most 24
+// significant bits left), so after one rounding of x to FP32 the split runs in FP32.
 template <int NT>
 __device__ __forceinline__ void split_terms(double x, __nv_bfloat16 (&t)[NT]) {
-    double r = x;
+    float r = (float)x;
 #pragma unroll
     for (int i = 0; i < NT; ++i) {
-        t[i] = __double2bfloat16(r);
-        r -= (double)__bfloat162float(t[i]);
+        t[i] = __float2bfloat16_rn(r);
+        r -= __bfloat162float(t[i]);
     }
 }
 
@@ -258,20 +260,38 @@ __global__ void __launch_bounds__(NTHREADS) k_tc_gemm(Args g) {
     int stage = 0;
     bool first = true;
     int abort_local = 0;  // this thread's bounded wait gave up; made block-uniform by __syncthreads_or
-    const int kq = (tid & 7) * 4;
+    // Item (row, 4 consecutive k) of a thread: for its j-th item the warp covers 16 rows of one
+    // 8-wide k octet -- lanes 0-7 rows 0-7 and lanes 8-15 the same rows' upper half of the
+    // octet, lanes 16-31 the next 8 rows -- so a warp's 8-byte stores into the core-matrix
+    // layout fill all 32 banks twice (two wavefronts, no conflict), and each pair of lanes reads
+    // 64 contiguous bytes of a row.
+    constexpr int NJA = BM * BK / 4 / NTHREADS, NJB = BN * BK / 4 / NTHREADS;
+    const int lrow = (lane & 7) + 8 * (lane >> 4), lk = ((lane >> 3) & 1) * 4;
+    auto item_a = [&](int j, int& r, int& k) {
+        const int c = j * (NTHREADS / 32) + warp;
+        r = (c % (BM / 16)) * 16 + lrow;
+        k = (c / (BM / 16)) * 8 + lk;
+    };
+    auto item_b = [&](int j, int& r, int& k) {
+        const int c = j * (NTHREADS / 32) + warp;
+        r = (c % (BN / 16)) * 16 + lrow;
+        k = (c / (BN / 16)) * 8 + lk;
+    };
     for (long kc = kbeg; kc < kend; kc += BK) {
         // FP64 loads of this chunk (issued before waiting for the stage to free up)
-        double va[BM * BK / 4 / NTHREADS][4];
-        double vb[(BN * BK / 4 + NTHREADS - 1) / NTHREADS][4];
+        double va[NJA][4];
+        double vb[NJB][4];
 #pragma unroll
-        for (int j = 0; j < BM * BK / 4 / NTHREADS; ++j) {
-            const int r = (tid >> 3) + j * (NTHREADS / 8);
-            load4(g.a, batch, (long)tm * BM + r, g.M, kc + kq, kend, va[j]);
+        for (int j = 0; j < NJA; ++j) {
+            int r, k;
+            item_a(j, r, k);
+            load4(g.a, batch, (long)tm * BM + r, g.M, kc + k, kend, va[j]);
         }
 #pragma unroll
-        for (int j = 0; j < (BN * BK / 4 + NTHREADS - 1) / NTHREADS; ++j) {
-            const int r = (tid >> 3) + j * (NTHREADS / 8);
-            if (r < BN) load4(g.b, batch, (long)tn * BN + r, g.N, kc + kq, kend, vb[j]);
+        for (int j = 0; j < NJB; ++j) {
+            int r, k;
+            item_b(j, r, k);
+            load4(g.b, batch, (long)tn * BN + r, g.N, kc + k, kend, vb[j]);
         }
         // the MMAs that last read this stage must be done
         if (stage == 0 && pend0) {
@@ -286,12 +306,16 @@ __global__ void __launch_bounds__(NTHREADS) k_tc_gemm(Args g) {
         uint8_t* sa = smem + stage * STAGE;
         uint8_t* sb = sa + NT * A_TERM;
 #pragma unroll
-        for (int j = 0; j < BM * BK / 4 / NTHREADS; ++j)
-            store_split<NT>(sa, A_TERM, (tid >> 3) + j * (NTHREADS / 8), kq, va[j]);
+        for (int j = 0; j < NJA; ++j) {
+            int r, k;
+            item_a(j, r, k);
+            store_split<NT>(sa, A_TERM, r, k, va[j]);
+        }
 #pragma unroll
-        for (int j = 0; j < (BN * BK / 4 + NTHREADS - 1) / NTHREADS; ++j) {
-            const int r = (tid >> 3) + j * (NTHREADS / 8);
-            if (r < BN) store_split<NT>(sb, B_TERM, r, kq, vb[j]);
+        for (int j = 0; j < NJB; ++j) {
+            int r, k;
+            item_b(j, r, k);
+            store_split<NT>(sb, B_TERM, r, k, vb[j]);
         }
         // generic-proxy stores -> visible to the tensor cores (async proxy)
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");

@@ -209,7 +209,7 @@ def run_reference(args) -> dict:
     rng = np.random.default_rng(0)
     # a density-like occupied block of the right size (cost does not depend on the values)
     Cw = np.linalg.qr(rng.standard_normal((ao.nao, mol.nelectron // 2)))[0] * np.sqrt(2.0)
-    stride = int(os.environ.get("DFB_REF_PAIR_STRIDE", "400"))
+    stride = int(os.environ.get("DFB_REF_PAIR_STRIDE", "100"))
     times = []
     for i in range(args.warmup + args.steps):
         r = ref_cpu.cpu_step(ao, aux, Cw, mol.natm, pair_stride=stride, threads=0)
@@ -430,7 +430,7 @@ def run_gpu(args) -> dict | None:
 
             if ref_cpu.available():
                 cores = os.cpu_count() or 1
-                stride = int(os.environ.get("DFB_REF_PAIR_STRIDE", "400"))
+                stride = int(os.environ.get("DFB_REF_PAIR_STRIDE", "100"))
                 r = ref_cpu.cpu_step(ao, aux, Cw.cpu().numpy(), mol.natm, pair_stride=stride)
                 out["cpu_baseline"] = {"value": round(1e3 * r["total"], 1), "unit": "ms", "cores": cores,
                                        "kind": "reference",
