@@ -53,19 +53,44 @@ def _nomark(_key: str) -> None:
     pass
 
 
-def df_forward(engine: DFEngine, Cw: torch.Tensor, precision: str = "fp64", X: torch.Tensor | None = None):
-    """Integrals at the engine's current geometry, then (E_2e, J, K) and the saved intermediates."""
+_JK_STREAMS: dict = {}
+
+
+def _jk_streams(device: torch.device):
+    """Two side streams per device: J (overlapping the metric solve) and K (overlapping the adjoints)."""
+    idx = device.index if device.index is not None else torch.cuda.current_device()
+    if idx not in _JK_STREAMS:
+        _JK_STREAMS[idx] = (torch.cuda.Stream(device=device), torch.cuda.Stream(device=device))
+    return _JK_STREAMS[idx]
+
+
+def _fork(main: torch.cuda.Stream, side: torch.cuda.Stream) -> None:
+    ev = torch.cuda.Event()
+    ev.record(main)
+    side.wait_event(ev)
+
+
+def df_forward(engine: DFEngine, Cw: torch.Tensor, precision: str = "fp64", X: torch.Tensor | None = None,
+               with_adjoints: bool = False):
+    """Integrals at the engine's current geometry, then (E_2e, J, K) and the saved intermediates
+    (with the gradient adjoints when ``with_adjoints``, see ``df_contract``)."""
     _V, L, X = engine.metric_cholesky_int3c(X, precision=precision)
-    return df_contract(engine, Cw, X, L, precision)
+    return df_contract(engine, Cw, X, L, precision, with_adjoints=with_adjoints)
 
 
 def df_contract(engine: DFEngine, Cw: torch.Tensor, X: torch.Tensor, L: torch.Tensor, precision: str = "fp64",
-                mark=_nomark):
+                mark=_nomark, with_adjoints: bool = False):
     """(E_2e, J, K) and the saved intermediates from the 3c tensor X ('Qmn') and the metric factor L.
 
     With D = Cw Cw^T the Coulomb density rho_P = <X_P, D> = sum Cw * (X_P Cw) is read
     from Y = X Cw (needed for K anyway) instead of a second pass over X.  ``mark(name)``
     is called after each phase (timing hooks).
+
+    J and K are off the critical path of the energy and gradient: J = sum_P d_P X_P runs on a
+    side stream while the main stream solves W = L^-1 Y, and K = sum W W^T on a second side
+    stream while the main stream forms the gradient adjoints (``with_adjoints``: Gamma written
+    over X, and G2, kept in the saved dict for ``df_backward``).  Both join the main stream
+    before this returns.
     """
     nao, naux = engine.nao, engine.naux
     nocc = Cw.shape[1]
@@ -80,8 +105,12 @@ def df_contract(engine: DFEngine, Cw: torch.Tensor, X: torch.Tensor, L: torch.Te
     mark("jk_Y")
     rho = Y @ Cw.reshape(-1)
     d = torch.cholesky_solve(rho.view(-1, 1), L).view(-1)
-    J = (d @ X2).view(nao, nao)
-    J = 0.5 * (J + J.T)
+    main = torch.cuda.current_stream(X.device)
+    sJ, sK = _jk_streams(X.device)
+    _fork(main, sJ)
+    with torch.cuda.stream(sJ):
+        J = (d @ X2).view(nao, nao)
+        J = 0.5 * (J + J.T)
     mark("jk_rho_J")
     # the solve stays FP64 in both modes: block substitution runs at the DGEMM rate, and a
     # split-BF16 product with L^-1 loses accuracy in proportion to the metric's conditioning
@@ -92,15 +121,22 @@ def df_contract(engine: DFEngine, Cw: torch.Tensor, X: torch.Tensor, L: torch.Te
     # M_Q = Cw^T W_Q (FP64 in both modes): the exchange energy tr(D K) = sum_Q |M_Q|^2, and the
     # adjoint's input
     M = torch.matmul(Cw.T, W3)
-    if mixed and MIXED_K_TC:
-        K = _tc.syrk_qblocks(W3)
-    else:
-        W2 = W3.permute(1, 0, 2).reshape(nao, naux * nocc)
-        K = W2 @ W2.T
-    K = 0.5 * (K + K.T)
+    _fork(main, sK)
+    with torch.cuda.stream(sK):
+        if mixed and MIXED_K_TC:
+            K = _tc.syrk_qblocks(W3)
+        else:
+            W2 = W3.permute(1, 0, 2).reshape(nao, naux * nocc)
+            K = W2 @ W2.T
+        K = 0.5 * (K + K.T)
     E = 0.5 * torch.dot(rho, d) - 0.25 * torch.sum(M * M)
+    saved = dict(X=X, L=L, d=d, W=W, M=M, D=D, Linv_blocks=Linv_blocks)
+    main.wait_stream(sJ)  # J has read X: the adjoint may overwrite it now
+    if with_adjoints:
+        saved["adj"] = df_adjoints(engine, Cw, saved, precision)
+    main.wait_stream(sK)
     mark("jk_K")
-    return E, J, K, dict(X=X, L=L, d=d, W=W, M=M, D=D, Linv_blocks=Linv_blocks)
+    return E, J, K, saved
 
 
 def df_adjoints(engine: DFEngine, Cw: torch.Tensor, saved: dict, precision: str = "fp64"):
@@ -131,7 +167,7 @@ def df_adjoints(engine: DFEngine, Cw: torch.Tensor, saved: dict, precision: str 
 def df_backward(engine: DFEngine, Cw: torch.Tensor, saved: dict, grad: torch.Tensor | None = None,
                 precision: str = "fp64") -> torch.Tensor:
     """dE_2e/dR accumulated into grad (natm, 3)."""
-    G3, G2 = df_adjoints(engine, Cw, saved, precision)
+    G3, G2 = saved["adj"] if "adj" in saved else df_adjoints(engine, Cw, saved, precision)
     if grad is None:
         grad = torch.zeros((engine.natm, 3), dtype=torch.float64, device=G3.device)
     engine.deriv3c_2c(G3, G2, grad, precision=precision)
@@ -144,7 +180,7 @@ class DFEnergyFunction(torch.autograd.Function):
     @staticmethod
     def forward(ctx, coords: torch.Tensor, Cw: torch.Tensor, engine: DFEngine, precision: str = "fp64"):
         engine.set_coords(coords.detach())
-        E, J, K, saved = df_forward(engine, Cw.detach(), precision)
+        E, J, K, saved = df_forward(engine, Cw.detach(), precision, with_adjoints=ctx.needs_input_grad[0])
         ctx.engine = engine
         ctx.precision = precision
         ctx.saved = saved

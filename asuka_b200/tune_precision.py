@@ -55,7 +55,7 @@ def _density(mol, eng):
 
 def _step(eng, Cw, R, X, precision):
     eng.set_coords(R)
-    E, _J, _K, saved = df_forward(eng, Cw, precision, X=X)
+    E, _J, _K, saved = df_forward(eng, Cw, precision, X=X, with_adjoints=True)
     g = df_backward(eng, Cw, saved, precision=precision)
     return float(E), g.cpu().numpy()
 

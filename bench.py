@@ -261,7 +261,7 @@ def run_gpu(args) -> dict | None:
 
     def step(prec):
         eng.set_coords(R)
-        E, J, K, saved = df_forward(eng, Cw, prec, X=X)
+        E, J, K, saved = df_forward(eng, Cw, prec, X=X, with_adjoints=True)
         g = df_backward(eng, Cw, saved, precision=prec)
         return E, g
 
