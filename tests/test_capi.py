@@ -27,3 +27,42 @@ def test_library_exports_every_declared_symbol():
     assert set(_declared()) <= set(_lib.exported_symbols()) | {n for n in _declared() if hasattr(L, n)}
     assert L.dfb_version() >= 100
     assert L.dfb_last_error() == b""
+
+
+def test_tensor_core_gemm_rejects_bad_arguments_without_a_gpu():
+    """Argument checks of dfb_tc_gemm run before any device call (their error codes and messages)."""
+    import ctypes
+
+    from asuka_b200 import _lib
+
+    L = _lib.lib()
+    a = _lib.TcOperand(0x1000, 4, 0, 1, 4, 0)
+    b = _lib.TcOperand(0x2000, 4, 0, 1, 4, 0)
+    cases = [
+        (dict(M=-1), "invalid arguments"),
+        (dict(nterms=4), "nterms"),
+        (dict(symmetric=1), "symmetric"),           # A != B
+        (dict(K=0), "K == 0"),
+        (dict(accumulate=0, kspan=32, K=100), "accumulate"),
+    ]
+    for over, msg in cases:
+        kw = dict(M=8, N=8, K=4, batch=1, accumulate=1, symmetric=0, nterms=3, kspan=0)
+        kw.update(over)
+        rc = L.dfb_tc_gemm(kw["M"], kw["N"], kw["K"], kw["batch"], ctypes.byref(a), ctypes.byref(b), 0x3000, 8, 0,
+                           kw["accumulate"], kw["symmetric"], kw["nterms"], kw["kspan"], None)
+        assert rc == -1, (over, rc)
+        assert msg in L.dfb_last_error().decode(), (over, L.dfb_last_error())
+    # empty products are a no-op
+    assert L.dfb_tc_gemm(0, 8, 4, 1, ctypes.byref(a), ctypes.byref(b), 0x3000, 8, 0, 1, 0, 3, 0, None) == 0
+
+
+def test_precision_entry_points_reject_unknown_precision_without_a_gpu():
+    import ctypes
+
+    from asuka_b200 import _lib
+
+    L = _lib.lib()
+    ps, ax = _lib.PairSide(), _lib.AuxSide()
+    rc = L.dfb_rys_int_prec(0, 0, 0, ctypes.byref(ps), ctypes.byref(ax), 0x10, 0x10, 0, 0, 0, 7, 0x10, 1, 1, 1, 0, 0,
+                            None)
+    assert rc == -1 and "precision" in L.dfb_last_error().decode()

@@ -1,4 +1,8 @@
-"""Active-space DF factors (CASSCF consumer) and streamed J/K with several occupied sets (UHF)."""
+"""Active-space DF factors (CASSCF consumer) and streamed J/K with several occupied sets (UHF).
+
+The active factors are checked against the same transform of the reference's own whitened
+factors (its 3c integrals and metric from the fixture) and, tighter, against the transform of
+this engine's B in every layout."""
 
 import numpy as np
 import pytest
@@ -29,9 +33,21 @@ def test_active_factors_all_layouts(name):
     ao, aux, eng, L, BQ = _stored(g)
     C = torch.as_tensor(g["mo_coeff"], device="cuda")[:, 2:8].contiguous()  # a 6-orbital active space
     norb, naux = C.shape[1], BQ.shape[0]
-    # plain reference: L[p q, Q] = sum_mn C_mp C_nq B_Q[m, n]
-    ref = np.einsum("mp,nq,Qmn->pqQ", C.cpu().numpy(), C.cpu().numpy(), BQ.cpu().numpy()).reshape(norb * norb, naux)
+    Ch = C.cpu().numpy()
+    # the reference's own factors: its unwhitened 3c integrals and metric from the fixture,
+    # whitened on the host (B = X L^-T), then L[p q, Q] = sum_mn C_mp C_nq B_Q[m, n]
+    from scipy.linalg import solve_triangular
+    from _util import unpack_tril
+
+    nao = Ch.shape[0]
+    Xr = unpack_tril(g["X_tril"], nao).reshape(nao * nao, naux)
+    Br = solve_triangular(np.linalg.cholesky(g["V"]), Xr.T, lower=True).T.reshape(nao, nao, naux)
+    ref_r = np.einsum("mp,nq,mnQ->pqQ", Ch, Ch, Br).reshape(norb * norb, naux)
+    ref = np.einsum("mp,nq,Qmn->pqQ", Ch, Ch, BQ.cpu().numpy()).reshape(norb * norb, naux)
     scale = np.abs(ref).max()
+    # this engine's whitened factors against the reference's (integrals ~1e-12, whitened through
+    # the metric's Cholesky factor)
+    assert np.abs(ref - ref_r).max() < 1e-9 * scale
     B_mnQ = BQ.permute(1, 2, 0).contiguous()
     for Lf in (active_Lfull_from_B(B_mnQ, C), active_Lfull_from_B(BQ, C, layout="Qmn"),
                active_Lfull_from_cached_B_whitened(B_mnQ, C),
@@ -41,6 +57,7 @@ def test_active_factors_all_layouts(name):
         assert np.abs(Lf.cpu().numpy() - ref).max() < 1e-12 * scale
     Ls = active_Lfull_streamed_basis(ao, aux, C, aux_block_naux=40)
     assert np.abs(Ls.cpu().numpy() - ref).max() < 1e-11 * scale
+    assert np.abs(Ls.cpu().numpy() - ref_r).max() < 1e-9 * scale
 
 
 @pytest.mark.parametrize("aux_block", [32, 100000])
