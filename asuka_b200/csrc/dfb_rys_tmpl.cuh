@@ -167,25 +167,6 @@ __device__ __forceinline__ void rys_eval_smem(const RysTable& tab, double T, dou
 
 // 2D recurrence tables of one root and direction in the component type R (double, or
 // float for the mixed-precision kernels; the coefficients arrive already rounded to R).
-// Table prefetch: the coefficient block of the next primitive triplet's T interval is requested
-// into L1 one triplet ahead (prefetch.global.L1: no registers, no shared memory), so the
-// gathers of the next root evaluation hit L1 instead of waiting on L2.  The interval only has
-// to be right to within a line, so T is formed in FP32.
-#ifndef DFB_TABLE_PREFETCH
-#define DFB_TABLE_PREFETCH 0
-#endif
-template <int NR>
-__device__ __forceinline__ void rys_prefetch(const RysTable& tab, float T) {
-    if (!(T < (float)tab.tmax)) return;
-    int k = (int)(T * (float)tab.inv_h);
-    if (k > tab.nint - 1) k = tab.nint - 1;
-    constexpr int BYTES = 2 * NR * (DFB_RYS_DEG + 1) * 8;
-    const char* c = reinterpret_cast<const char*>(tab.coef + tab.offs[NR] + (size_t)k * (2 * NR) * (DFB_RYS_DEG + 1));
-#pragma unroll
-    for (int off = 0; off < BYTES; off += 128) asm volatile("prefetch.global.L1 [%0];" ::"l"(c + off));
-    asm volatile("prefetch.global.L1 [%0];" ::"l"(c + BYTES - 8));
-}
-
 template <int NM, int MM, typename R>
 __device__ __forceinline__ void build_G_t(R (&G)[NM + 1][MM + 1], R g00, R C, R Cp, R B0, R B1, R B1p) {
     G[0][0] = g00;
@@ -490,17 +471,6 @@ __device__ __forceinline__ void rys_thread_body(const TmplArgs& g, long task, do
             const double cc = g.ax.pcoef[c0 + ic];
             const double inv = 1.0 / (p + q);
             const double T = p * q * inv * PQ2;
-#if DFB_TABLE_PREFETCH
-            if (ic + 1 < nc) {
-                const float qn = (float)g.ax.pexp[c0 + ic + 1];
-                rys_prefetch<NR>(g.tab, __fdividef((float)p * qn, (float)p + qn) * (float)PQ2);
-            } else if (iab + 1 < nab) {
-                const float pn = (float)g.ps.eta[p0 + iab + 1], qn = (float)g.ax.pexp[c0];
-                const float dx = (float)(Cc[0] - g.ps.Px[p0 + iab + 1]), dy = (float)(Cc[1] - g.ps.Py[p0 + iab + 1]);
-                const float dz = (float)(Cc[2] - g.ps.Pz[p0 + iab + 1]);
-                rys_prefetch<NR>(g.tab, __fdividef(pn * qn, pn + qn) * (dx * dx + dy * dy + dz * dz));
-            }
-#endif
             const double pref = kTwoPi52_t / (p * q * sqrt(p + q)) * cK * cc;
             // few roots: registers; more roots: shared-memory slot (bounds registers)
             constexpr int NRR = NR <= 2 ? NR : 1;

@@ -38,7 +38,6 @@ _DATA = os.path.join(os.path.dirname(os.path.abspath(__file__)), "data")
 _TABLE_READY: set[int] = set()
 PRIM_SCREEN = 1e-20  # primitive-pair magnitude bound below which a pair is skipped (0 = evaluate all)
 NSTREAMS = int(os.environ.get("DFB_STREAMS", "8"))  # side streams for per-class launches (2/4/6/8 measured: 8 fastest)
-LPT = os.environ.get("DFB_LPT", "1") != "0"  # longest-first class scheduling over the side streams
 NROOTS_SLOTS = 11  # DFB_NROOTS_MAX + 1
 _SIDE_STREAMS: dict[int, list] = {}
 
@@ -211,14 +210,11 @@ class DFEngine:
         P = np.where(swap, Qi, Pi)
         Q = np.where(swap, Pi, Qi)
         lP, lQ = aux_l[P], aux_l[Q]
-        self._cost2c = {}  # (lP, lQ) -> primitive pairs of the class (launch-order cost estimate)
         for a in np.unique(lP):
             for c in np.unique(lQ):
                 sel = np.nonzero((lP == a) & (lQ == c))[0]
                 if sel.size:
                     self.classes2c.append((int(a), int(c), i32(P[sel]), i32(Q[sel])))
-                    self._cost2c[(int(a), int(c))] = float(
-                        (aux.shell_nprim[P[sel]].astype(np.float64) * aux.shell_nprim[Q[sel]]).sum())
         self._scratch = scratch if scratch is not None else ScratchHolder()
         self._build_ao_pairs(ao.shell_cxyz)
         self._build_pair_tables()
@@ -232,20 +228,9 @@ class DFEngine:
             _SIDE_STREAMS[idx] = [torch.cuda.Stream(device=self.device) for _ in range(NSTREAMS)]
         return _SIDE_STREAMS[idx]
 
-    def class_cost(self, la: int, lb: int, lc: int, deriv: bool, metric: bool = False) -> float:
-        """Work estimate of one class launch: primitive triplets x Rys roots x (the survey's
-        per-unit product count + recurrence tables); orders the launches over the side streams."""
-        nf = ncart(la) * ncart(lb) * ncart(lc)
-        nr = (la + lb + lc + (1 if deriv else 0)) // 2 + 1
-        per = nf * (25 if deriv else 3) + 9 * (la + lb + 1 + deriv) * (lc + 1 + deriv)
-        if metric:
-            return self._cost2c.get((la, lc), 0.0) * nr * per
-        return self._kab.get((la, lb), 0.0) * self._kp.get(lc, 0.0) * nr * per
-
-    def _fanout(self, launches, costs=None):
-        """Run launch(stream_ptr) callables over the side streams, ordered after and before the
-        current stream.  With ``costs``, longest first, each onto the side stream with the least
-        work so far (so the heavy classes do not queue behind each other); else round-robin."""
+    def _fanout(self, launches):
+        """Run launch(stream_ptr) callables round-robin over side streams, ordered after and
+        before the current stream."""
         main = torch.cuda.current_stream(self.device)
         side = self._streams() if NSTREAMS > 1 else [main]
         if NSTREAMS > 1:
@@ -253,15 +238,8 @@ class DFEngine:
             start.record(main)
             for st in side:
                 st.wait_event(start)
-        if costs is None or not LPT or len(side) == 1:
-            for i, fn in enumerate(launches):
-                fn(int(side[i % len(side)].cuda_stream))
-        else:
-            load = [0.0] * len(side)
-            for i in sorted(range(len(launches)), key=lambda i: -costs[i]):
-                s = min(range(len(side)), key=lambda k: load[k])
-                load[s] += costs[i]
-                launches[i](int(side[s].cuda_stream))
+        for i, fn in enumerate(launches):
+            fn(int(side[i % len(side)].cuda_stream))
         if NSTREAMS > 1:
             for st in side:
                 ev = torch.cuda.Event()
@@ -324,14 +302,11 @@ class DFEngine:
         # dropped shell pairs write nothing: outputs are zero-filled first when any exist
         self.n_dropped_pairs = int((~live).sum())
         self.classes3c = []  # (la, lb, lc, pairs tensor, aux tensor)
-        self._kab = {}  # (la, lb) -> kept primitive pairs of the class
-        self._kp = {int(l): float(self.aux.shell_nprim[self.aux.shell_l == l].sum()) for l in self.aux_by_l}
         for a in np.unique(la):
             for b in np.unique(lb):
                 sel = np.nonzero((la == a) & (lb == b) & live)[0]
                 if sel.size == 0:
                     continue
-                self._kab[(int(a), int(b))] = float(cnt[sel].sum())
                 # pairs by decreasing primitive-pair count: with the aux-major task
                 # grid a warp walks pairs of similar cost against one aux shell
                 sel = sel[np.argsort(-cnt[sel], kind="stable")]
@@ -516,8 +491,7 @@ class DFEngine:
         V = out if out is not None else torch.empty((naux, naux), dtype=torch.float64, device=self.device)
         self._slices_int = self._scratch_slices(False)
         self._fanout([self._launch_int(lp, 0, lq, self.ps_aux, self.axs, P, Q, P.numel(), 0, 1, V, (naux, 1, 0))
-                      for lp, lq, P, Q in self.classes2c],
-                     [self.class_cost(lp, 0, lq, False, metric=True) for lp, lq, _P, _Q in self.classes2c])
+                      for lp, lq, P, Q in self.classes2c])
         # diagonal shell blocks are written from one tile in both orders; make V
         # exactly symmetric as the reference does (cueri_df_cpu.py: V = (V+V^T)/2)
         V.copy_(0.5 * (V + V.T))
@@ -541,8 +515,7 @@ class DFEngine:
         self._slices_int = self._scratch_slices(False)
         pc = _prec_code(precision)
         self._fanout([self._launch_int(la, lb, lc, self.ps_ao, self.axs, pairs, auxs, pairs.numel() * auxs.numel(),
-                                       -pairs.numel(), 0, X, s, pc) for la, lb, lc, pairs, auxs in self.classes3c],
-                     [self.class_cost(la, lb, lc, False) for la, lb, lc, _p, _a in self.classes3c])
+                                       -pairs.numel(), 0, X, s, pc) for la, lb, lc, pairs, auxs in self.classes3c])
         return X
 
     def deriv3c(self, bar: torch.Tensor, grad: torch.Tensor, layout: str = "Qmn", precision: str = "fp64") -> torch.Tensor:
@@ -559,8 +532,7 @@ class DFEngine:
         pc = _prec_code(precision)
         self._fanout([self._launch_deriv(la, lb, lc, self.ps_ao, self.axs, pairs, auxs, pairs.numel() * auxs.numel(),
                                          -pairs.numel(), 0, bar, s, grad, pc)
-                      for la, lb, lc, pairs, auxs in self.classes3c],
-                     [self.class_cost(la, lb, lc, True) for la, lb, lc, _p, _a in self.classes3c])
+                      for la, lb, lc, pairs, auxs in self.classes3c])
         return grad
 
     def deriv2c(self, bar: torch.Tensor, grad: torch.Tensor, precision: str = "fp64") -> torch.Tensor:
@@ -570,8 +542,7 @@ class DFEngine:
         self._slices_der = self._scratch_slices(True)
         pc = _prec_code(precision)
         self._fanout([self._launch_deriv(lp, 0, lq, self.ps_aux, self.axs, P, Q, P.numel(), 0, 1, bar, (naux, 1, 0),
-                                         grad, pc) for lp, lq, P, Q in self.classes2c],
-                     [self.class_cost(lp, 0, lq, True, metric=True) for lp, lq, _P, _Q in self.classes2c])
+                                         grad, pc) for lp, lq, P, Q in self.classes2c])
         return grad
 
 
@@ -611,20 +582,8 @@ class DFEngine:
             ev = torch.cuda.Event()
             ev.record(st)
             main.wait_event(ev)
-        if LPT:
-            # the 3c classes longest first, each onto the least-loaded side stream
-            c2 = [self.class_cost(lp, 0, lq, False, metric=True) for lp, lq, _P, _Q in self.classes2c]
-            load = [0.0] * len(side)
-            for i, c in enumerate(c2):
-                load[i % len(side)] += c
-            c3 = [self.class_cost(la, lb, lc, False) for la, lb, lc, _p, _a in self.classes3c]
-            for i in sorted(range(len(second)), key=lambda i: -c3[i]):
-                s = min(range(len(side)), key=lambda k: load[k])
-                load[s] += c3[i]
-                second[i](int(side[s].cuda_stream))
-        else:
-            for i, fn in enumerate(second):
-                fn(int(side[(i + len(first)) % len(side)].cuda_stream))
+        for i, fn in enumerate(second):
+            fn(int(side[(i + len(first)) % len(side)].cuda_stream))
         V.copy_(0.5 * (V + V.T))
         L, info = torch.linalg.cholesky_ex(V)
         for st in side:
@@ -648,9 +607,7 @@ class DFEngine:
                     for la, lb, lc, pairs, auxs in self.classes3c]
         launches += [self._launch_deriv(lp, 0, lq, self.ps_aux, self.axs, P, Q, P.numel(), 0, 1, bar2, (naux, 1, 0),
                                         grad, pc) for lp, lq, P, Q in self.classes2c]
-        costs = [self.class_cost(la, lb, lc, True) for la, lb, lc, _p, _a in self.classes3c]
-        costs += [self.class_cost(lp, 0, lq, True, metric=True) for lp, lq, _P, _Q in self.classes2c]
-        self._fanout(launches, costs)
+        self._fanout(launches)
         return grad
 
 
