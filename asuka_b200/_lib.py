@@ -27,7 +27,7 @@ class TcOperand(ctypes.Structure):
 
 
 class AuxSide(ctypes.Structure):
-    _fields_ = [(n, ctypes.c_void_p) for n in ("cxyz", "pstart", "nprim", "pexp", "pcoef", "aostart", "atom")]
+    _fields_ = [(n, ctypes.c_void_p) for n in ("cxyz", "pstart", "nprim", "pexp", "pcoef", "rexp", "aostart", "atom")]
 
 
 _SIGS = {

@@ -54,8 +54,8 @@ __device__ __forceinline__ void task_indices(long t, long grid, long& tp, long& 
 __device__ __forceinline__ void rys_eval(const RysTable& tab, int n, double T, double* x, double* w, int xs = 1) {
     if (T >= tab.tmax) {
         const double* h = tab.herm + tab.hoff[n];
-        const double inv = 1.0 / T;
         const double rs = rsqrt(T);
+        const double inv = rs * rs;
         for (int i = 0; i < n; ++i) {
             x[i * xs] = __ldg(h + i) * inv;
             w[i * xs] = __ldg(h + n + i) * rs;

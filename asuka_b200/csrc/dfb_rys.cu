@@ -51,6 +51,19 @@ struct ClassInfo {
     int item;        // doubles per primitive-triplet record
 };
 
+// Fields of one primitive triplet's shared-memory record in the generic path (field f of
+// lane j at items[32 f + j]): everything the per-root recurrence coefficients need, with the
+// reciprocals taken once per triplet, then the nodes and the prefactor-scaled weights.
+enum {
+    DFB_REC_HINV = 0,  // 1 / (2 (p+q))
+    DFB_REC_HP = 1,    // 1 / (2p)
+    DFB_REC_HQ = 2,    // 1 / (2q)
+    DFB_REC_PA = 3,    // P - A (3 fields)
+    DFB_REC_QCP = 6,   // q/(p+q) (C - P) (3 fields)
+    DFB_REC_PCP = 9,   // -p/(p+q) (C - P) (3 fields)
+    DFB_REC_X = 12     // nodes (nr fields), then weights x prefactor (nr fields)
+};
+
 static ClassInfo make_class(int la, int lb, int lc, bool deriv) {
     ClassInfo c;
     c.la = la;
@@ -68,9 +81,10 @@ static ClassInfo make_class(int la, int lb, int lc, bool deriv) {
     c.nb = ncart(lb);
     c.nc = ncart(lc);
     c.gt = (c.nmax + 1) * (c.mmax + 1);
-    c.item = 8 + 2 * c.nr;
+    c.item = DFB_REC_X + 2 * c.nr;
     return c;
 }
+
 
 __device__ __forceinline__ void decode_cart(int l, int idx, int& x, int& y, int& z) {
     int xx = l;
@@ -207,23 +221,29 @@ __global__ void __launch_bounds__(DFB_WARPS_PER_BLOCK * 32, DFB_ACC_MIN_BLOCKS)
                 const double p = ps.eta[p0 + iab];
                 const double Pp[3] = {ps.Px[p0 + iab], ps.Py[p0 + iab], ps.Pz[p0 + iab]};
                 const double q = ax.pexp[c0 + ic];
-                const double inv = 1.0 / (p + q);
+                const double rp = 1.0 / p, rq = ax.rexp[c0 + ic];
+                // one reciprocal square root: 1/(p+q) = s^2, 1/(p q sqrt(p+q)) = rp rq s
+                const double s = rsqrt(p + q);
+                const double inv = s * s;
+                const double qi = q * inv, pi = p * inv;
                 double PQ2 = 0.0;
                 double* it = items + lane;  // field f of this lane's record at it[32 f]
-                it[0] = p;
-                it[32] = q;
+                it[32 * DFB_REC_HINV] = 0.5 * inv;
+                it[32 * DFB_REC_HP] = 0.5 * rp;
+                it[32 * DFB_REC_HQ] = 0.5 * rq;
 #pragma unroll
                 for (int d = 0; d < 3; ++d) {
                     const double cp = Cc[d] - Pp[d];
                     PQ2 += cp * cp;
-                    it[32 * (2 + d)] = Pp[d] - A[d];
-                    it[32 * (5 + d)] = cp;
+                    it[32 * (DFB_REC_PA + d)] = Pp[d] - A[d];
+                    it[32 * (DFB_REC_QCP + d)] = qi * cp;
+                    it[32 * (DFB_REC_PCP + d)] = -pi * cp;
                 }
                 const double T = p * q * inv * PQ2;
-                const double pref = kTwoPi52 / (p * q * sqrt(p + q)) * ps.cK[p0 + iab] * ax.pcoef[c0 + ic];
+                const double pref = kTwoPi52 * ps.cK[p0 + iab] * rp * (ax.pcoef[c0 + ic] * rq) * s;
                 // nodes and weights straight into the lane's shared-memory record
-                rys_eval(tab, ci.nr, T, it + 32 * 8, it + 32 * (8 + ci.nr), 32);
-                for (int u = 0; u < ci.nr; ++u) it[32 * (8 + ci.nr + u)] *= pref;
+                rys_eval(tab, ci.nr, T, it + 32 * DFB_REC_X, it + 32 * (DFB_REC_X + ci.nr), 32);
+                for (int u = 0; u < ci.nr; ++u) it[32 * (DFB_REC_X + ci.nr + u)] *= pref;
             }
             __syncwarp();
             const int nb = (int)((nitems - base) < 32 ? (nitems - base) : 32);
@@ -231,15 +251,13 @@ __global__ void __launch_bounds__(DFB_WARPS_PER_BLOCK * 32, DFB_ACC_MIN_BLOCKS)
                 const double* it = items + jj;
                 if (lane < ci.nr * 3) {
                     const int u = lane / 3, d = lane - 3 * (lane / 3);
-                    const double p = it[0], q = it[32];
-                    const double inv = 1.0 / (p + q);
-                    const double x = it[32 * (8 + u)];
-                    const double B0 = x * 0.5 * inv;
-                    const double B1 = (1.0 - x) * 0.5 / p + B0;
-                    const double B1p = (1.0 - x) * 0.5 / q + B0;
-                    const double Cd = it[32 * (2 + d)] + (q * inv) * x * it[32 * (5 + d)];
-                    const double Cpd = -(p * inv) * x * it[32 * (5 + d)];
-                    const double g00 = (d == 0) ? it[32 * (8 + ci.nr + u)] : 1.0;
+                    const double x = it[32 * (DFB_REC_X + u)];
+                    const double B0 = x * it[32 * DFB_REC_HINV];
+                    const double B1 = (1.0 - x) * it[32 * DFB_REC_HP] + B0;
+                    const double B1p = (1.0 - x) * it[32 * DFB_REC_HQ] + B0;
+                    const double Cd = it[32 * (DFB_REC_PA + d)] + x * it[32 * (DFB_REC_QCP + d)];
+                    const double Cpd = x * it[32 * (DFB_REC_PCP + d)];
+                    const double g00 = (d == 0) ? it[32 * (DFB_REC_X + ci.nr + u)] : 1.0;
                     build_G(gtab + (u * 3 + d) * ci.gt, ci.nmax, ci.mmax, g00, Cd, Cpd, B0, B1, B1p);
                 }
                 __syncwarp();
@@ -631,6 +649,8 @@ static int dispatch_rys(int la, int lb, int lc, const dfb_pair_side_t* ps, const
         return set_error(DFB_ERR_UNSUPPORTED, "angular momentum out of range (la=%d lb=%d lc=%d, max %d)", la, lb, lc,
                          DFB_LMAX);
     if (lb > la) return set_error(DFB_ERR_INVALID, "pairs must be l-ordered (la >= lb)");
+    if (!query_only && ntask > 0 && (!ax->pexp || !ax->pcoef || !ax->rexp))
+        return set_error(DFB_ERR_INVALID, "aux side without exponents, coefficients or reciprocal exponents");
     const ClassInfo ci = make_class(la, lb, lc, DERIV);
     if (ci.nr > DFB_NROOTS_MAX) return set_error(DFB_ERR_UNSUPPORTED, "too many Rys roots (%d)", ci.nr);
     const int dev = current_device();

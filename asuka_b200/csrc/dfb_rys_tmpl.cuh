@@ -90,8 +90,8 @@ template <int NR>
 __device__ __forceinline__ void rys_eval_t(const RysTable& tab, double T, double (&x)[NR], double (&w)[NR]) {
     if (T >= tab.tmax) {
         const double* h = tab.herm + tab.hoff[NR];
-        const double inv = 1.0 / T;
         const double rs = rsqrt(T);
+        const double inv = rs * rs;
 #pragma unroll
         for (int i = 0; i < NR; ++i) {
             x[i] = __ldg(h + i) * inv;
@@ -132,8 +132,8 @@ template <int NR, int RS>
 __device__ __forceinline__ void rys_eval_smem(const RysTable& tab, double T, double* __restrict__ r) {
     if (T >= tab.tmax) {
         const double* h = tab.herm + tab.hoff[NR];
-        const double inv = 1.0 / T;
         const double rs = rsqrt(T);
+        const double inv = rs * rs;
 #pragma unroll
         for (int i = 0; i < NR; ++i) {
             r[i * RS] = __ldg(h + i) * inv;
@@ -453,9 +453,14 @@ __device__ __forceinline__ void rys_thread_body(const TmplArgs& g, long task, do
     typename CL::Acc acc;
     CL::zero(acc);
 
+    // No division in the primitive loops: 1/p once per primitive pair, 1/q from the aux
+    // table, and one reciprocal square root s = (p+q)^(-1/2) per primitive triplet, with
+    // 1/(p+q) = s^2 and the prefactor 2 pi^(5/2) / (p q sqrt(p+q)) = (2 pi^(5/2) cK / p) (cc / q) s.
     for (int iab = 0; iab < nab; ++iab) {
         const double p = g.ps.eta[p0 + iab];
-        const double cK = g.ps.cK[p0 + iab];
+        const double rp = 1.0 / p;
+        const double cKr = kTwoPi52_t * g.ps.cK[p0 + iab] * rp;
+        const double h_p = 0.5 * rp;
         const R a2 = CL::DERIV ? (R)(2.0 * g.ps.ea[p0 + iab]) : R(0);
         const R b2 = CL::DERIV ? (R)(2.0 * g.ps.eb[p0 + iab]) : R(0);
         const double Pp[3] = {g.ps.Px[p0 + iab], g.ps.Py[p0 + iab], g.ps.Pz[p0 + iab]};
@@ -468,10 +473,11 @@ __device__ __forceinline__ void rys_thread_body(const TmplArgs& g, long task, do
         }
         for (int ic = 0; ic < nc; ++ic) {
             const double q = g.ax.pexp[c0 + ic];
-            const double cc = g.ax.pcoef[c0 + ic];
-            const double inv = 1.0 / (p + q);
+            const double rq = g.ax.rexp[c0 + ic];
+            const double s = rsqrt(p + q);
+            const double inv = s * s;
             const double T = p * q * inv * PQ2;
-            const double pref = kTwoPi52_t / (p * q * sqrt(p + q)) * cK * cc;
+            const double pref = cKr * (g.ax.pcoef[c0 + ic] * rq) * s;
             // few roots: registers; more roots: shared-memory slot (bounds registers)
             constexpr int NRR = NR <= 2 ? NR : 1;
             double xr[NRR], wr[NRR];
@@ -480,7 +486,7 @@ __device__ __forceinline__ void rys_thread_body(const TmplArgs& g, long task, do
             else
                 rys_eval_smem<NR, RS>(g.tab, T, sroot);
             const double qi = q * inv, pi = p * inv;
-            const double h_p = 0.5 / p, h_q = 0.5 / q;
+            const double h_q = 0.5 * rq;
 #pragma unroll
             for (int u = 0; u < NR; ++u) {
                 double x, wu;

@@ -185,6 +185,7 @@ class DFEngine:
         self.ax_nprim = i32(aux.shell_nprim)
         self.ax_exp = f64(aux.prim_exp)
         self.ax_coef = f64(aux.prim_coef)
+        self.ax_rexp = f64(1.0 / np.asarray(aux.prim_exp, dtype=np.float64))
         self.ax_aostart = i32(aux.shell_ao_start)
         self.ax_atom = i32(aux.shell_atom)
         self.ax_self = i32(np.arange(aux.nshell, dtype=np.int32))
@@ -194,12 +195,12 @@ class DFEngine:
             *[_lib.ptr(t) for t in (self.ax_self, self.ax_self, self.ax_pstart, self.ax_nprim, *self.axpt,
                                     self.ax_cxyz, self.ax_aostart, self.ax_atom)], 1)
         self.axs = _lib.AuxSide(*[_lib.ptr(t) for t in (self.ax_cxyz, self.ax_pstart, self.ax_nprim, self.ax_exp,
-                                                        self.ax_coef, self.ax_aostart, self.ax_atom)])
+                                                        self.ax_coef, self.ax_rexp, self.ax_aostart, self.ax_atom)])
         aux_l = aux.shell_l
         self.aux_by_l = {}
         for l in np.unique(aux_l):
             idx = np.nonzero(aux_l == l)[0]
-            idx = idx[np.argsort(aux.shell_nprim[idx], kind="stable")]
+            idx = idx[np.argsort(-aux.shell_nprim[idx], kind="stable")]
             self.aux_by_l[int(l)] = i32(idx)
         # metric classes: unordered aux pairs oriented l(P) >= l(Q)
         self.classes2c = []
@@ -384,7 +385,7 @@ class DFEngine:
             p1 = p0 + int(tot)
             shifted = torch.as_tensor(aux.shell_ao_start.astype(np.int32) - p0, device=self.device)
             axb = _lib.AuxSide(*[_lib.ptr(t) for t in (self.ax_cxyz, self.ax_pstart, self.ax_nprim, self.ax_exp,
-                                                       self.ax_coef, shifted, self.ax_atom)])
+                                                       self.ax_coef, self.ax_rexp, shifted, self.ax_atom)])
             byl = {}
             for l in np.unique(aux.shell_l[s0:s1]):
                 idx = s0 + np.nonzero(aux.shell_l[s0:s1] == l)[0]

@@ -29,6 +29,7 @@ typedef struct {
     const double *cxyz;
     const int *pstart, *nprim;
     const double *pexp, *pcoef;
+    const double *rexp;            /* 1 / pexp per primitive (the kernels' inner loops divide by nothing) */
     const int *aostart;
     const int *atom;
 } dfb_aux_side_t;
