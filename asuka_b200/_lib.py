@@ -57,6 +57,8 @@ _SIGS = {
                                                           ctypes.c_long, ctypes.c_long, ctypes.c_int, ctypes.c_int,
                                                           ctypes.c_int, ctypes.c_long, _d]),
     "dfb_tc_error": (ctypes.c_int, [ctypes.c_int]),
+    "dfb_gamma_sym": (ctypes.c_int, [ctypes.c_long, ctypes.c_int, ctypes.c_int, _d, ctypes.c_long, ctypes.c_long,
+                                     _d, _d, _d]),
     "dfb_fp32_fma_probe": (ctypes.c_int, [_d, ctypes.c_int, ctypes.c_int, ctypes.c_int, _d]),
     "dfb_launch_count": (ctypes.c_long, []),
     "dfb_rys_scratch_doubles": (ctypes.c_long, [ctypes.c_int] * 3 + [ctypes.c_long, ctypes.c_int]),

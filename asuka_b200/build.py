@@ -57,6 +57,22 @@ def _local_includes(path: str, seen: set | None = None) -> set:
     return seen
 
 
+def _same_as_main(src: str, srcdir: str) -> bool:
+    """True when ``src`` (in a generated copy of csrc) and every header it includes from that
+    copy are byte-identical to the main tree's files, whose object is then up to date."""
+
+    def read(p):
+        with open(p, "rb") as f:
+            return f.read()
+
+    for p in [src, *_local_includes(src)]:
+        rel = os.path.relpath(p, srcdir)
+        main = os.path.normpath(os.path.join(CSRC, rel))
+        if not os.path.exists(main) or read(p) != read(main):
+            return False
+    return os.path.exists(os.path.join(HERE, "_build", os.path.basename(src)[:-3] + ".o"))
+
+
 def _wait_slot(procs: list, jobs: int) -> None:
     """Block until fewer than ``jobs`` of the compiler processes are still running."""
     while sum(1 for p in procs if p.poll() is None) >= jobs:
@@ -111,8 +127,9 @@ def build_variant(defines: list[str], out: str, tag: str, jobs: int | None = Non
 
     ``defines``: extra -D flags for the class-specialised kernels, the other sources reuse
     the main build's objects.  ``gen_env``: regenerate the class kernels under these
-    environment variables (e.g. another accumulator budget) in a copy of csrc and build
-    every source of that copy (the dispatcher depends on the generated class set).
+    environment variables (e.g. another accumulator budget) in a copy of csrc and build the
+    sources of that copy; a source whose text and included headers are byte-identical to the
+    main tree's reuses the main build's object.
     """
     import shutil
 
@@ -129,14 +146,15 @@ def build_variant(defines: list[str], out: str, tag: str, jobs: int | None = Non
         srcdir = os.path.join(vdir, "src")
         if os.path.exists(srcdir):
             shutil.rmtree(srcdir)
-        shutil.copytree(CSRC, srcdir, ignore=shutil.ignore_patterns("class_tuning.json", "__pycache__"))
+        shutil.copytree(CSRC, srcdir, ignore=shutil.ignore_patterns("__pycache__"))
         env = dict(os.environ, **gen_env)
         subprocess.run([sys.executable, os.path.join(srcdir, "gen_classes.py"), srcdir], check=True, env=env)
     objs, procs = [], []
     jobs = jobs or max(1, os.cpu_count() or 1)
     for src in sorted(glob.glob(os.path.join(srcdir, "*.cu"))):
         base = os.path.basename(src)[:-3]
-        if not gen_env and not base.startswith("dfb_cls_"):
+        if (not gen_env and not base.startswith("dfb_cls_")) or (gen_env and not defines
+                                                                 and _same_as_main(src, srcdir)):
             objs.append(os.path.join(objdir, base + ".o"))
             continue
         obj = os.path.join(vdir, base + ".o")

@@ -12,7 +12,7 @@ int dfb_cls_d00_launch(int lc, const TmplArgs& g, long nblk, size_t smem, cudaSt
         return 1;
     }
     if (lc == 2) {
-        k_rys_thread<0, 0, 2, 2, true, false, 1, double><<<dim3((unsigned)nblk, 2), 128, smem, st>>>(g);
+        k_rys_thread<0, 0, 2, 1, true, false, 1, double><<<dim3((unsigned)nblk, 1), 128, smem, st>>>(g);
         return 1;
     }
     if (lc == 3) {
@@ -28,7 +28,7 @@ int dfb_cls_d00_launch(int lc, const TmplArgs& g, long nblk, size_t smem, cudaSt
         return 1;
     }
     if (lc == 6) {
-        k_rys_thread<0, 0, 6, 6, true, false, 1, double><<<dim3((unsigned)nblk, 6), 128, smem, st>>>(g);
+        k_rys_thread<0, 0, 6, 3, true, false, 1, double><<<dim3((unsigned)nblk, 3), 128, smem, st>>>(g);
         return 1;
     }
     return 0;

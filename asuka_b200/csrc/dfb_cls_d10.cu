@@ -8,7 +8,7 @@ int dfb_cls_d10_launch(int lc, const TmplArgs& g, long nblk, size_t smem, cudaSt
         return 1;
     }
     if (lc == 1) {
-        k_rys_thread<1, 0, 1, 2, true, false, 1, double><<<dim3((unsigned)nblk, 2), 128, smem, st>>>(g);
+        k_rys_thread<1, 0, 1, 1, true, false, 1, double><<<dim3((unsigned)nblk, 1), 128, smem, st>>>(g);
         return 1;
     }
     if (lc == 2) {
@@ -16,7 +16,7 @@ int dfb_cls_d10_launch(int lc, const TmplArgs& g, long nblk, size_t smem, cudaSt
         return 1;
     }
     if (lc == 3) {
-        k_rys_thread<1, 0, 3, 3, true, false, 1, double><<<dim3((unsigned)nblk, 3), 128, smem, st>>>(g);
+        k_rys_thread<1, 0, 3, 4, true, false, 1, double><<<dim3((unsigned)nblk, 4), 128, smem, st>>>(g);
         return 1;
     }
     if (lc == 4) {
@@ -28,7 +28,7 @@ int dfb_cls_d10_launch(int lc, const TmplArgs& g, long nblk, size_t smem, cudaSt
         return 1;
     }
     if (lc == 6) {
-        k_rys_thread<1, 0, 6, 7, true, false, 1, double><<<dim3((unsigned)nblk, 7), 128, smem, st>>>(g);
+        k_rys_thread<1, 0, 6, 10, true, false, 1, double><<<dim3((unsigned)nblk, 10), 128, smem, st>>>(g);
         return 1;
     }
     return 0;

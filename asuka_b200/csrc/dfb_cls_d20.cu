@@ -16,7 +16,7 @@ int dfb_cls_d20_launch(int lc, const TmplArgs& g, long nblk, size_t smem, cudaSt
         return 1;
     }
     if (lc == 3) {
-        k_rys_thread<2, 0, 3, 5, true, false, 1, double><<<dim3((unsigned)nblk, 5), 128, smem, st>>>(g);
+        k_rys_thread<2, 0, 3, 4, true, false, 1, double><<<dim3((unsigned)nblk, 4), 128, smem, st>>>(g);
         return 1;
     }
     if (lc == 4) {

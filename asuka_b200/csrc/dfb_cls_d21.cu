@@ -4,7 +4,7 @@
 namespace dfb {
 int dfb_cls_d21_launch(int lc, const TmplArgs& g, long nblk, size_t smem, cudaStream_t st) {
     if (lc == 0) {
-        k_rys_thread<2, 1, 0, 1, true, true, 1, double><<<dim3((unsigned)nblk, 2), 128, smem, st>>>(g);
+        k_rys_thread<2, 1, 0, 1, true, false, 1, double><<<dim3((unsigned)nblk, 1), 128, smem, st>>>(g);
         return 1;
     }
     if (lc == 1) {

@@ -12,7 +12,7 @@ int dfb_cls_d30_launch(int lc, const TmplArgs& g, long nblk, size_t smem, cudaSt
         return 1;
     }
     if (lc == 2) {
-        k_rys_thread<3, 0, 2, 6, true, false, 1, double><<<dim3((unsigned)nblk, 6), 128, smem, st>>>(g);
+        k_rys_thread<3, 0, 2, 3, true, false, 1, double><<<dim3((unsigned)nblk, 3), 128, smem, st>>>(g);
         return 1;
     }
     if (lc == 3) {
@@ -20,7 +20,7 @@ int dfb_cls_d30_launch(int lc, const TmplArgs& g, long nblk, size_t smem, cudaSt
         return 1;
     }
     if (lc == 4) {
-        k_rys_thread<3, 0, 4, 8, true, true, 1, double><<<dim3((unsigned)nblk, 16), 128, smem, st>>>(g);
+        k_rys_thread<3, 0, 4, 15, true, false, 1, double><<<dim3((unsigned)nblk, 15), 128, smem, st>>>(g);
         return 1;
     }
     if (lc == 5) {

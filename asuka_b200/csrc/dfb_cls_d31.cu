@@ -8,23 +8,23 @@ int dfb_cls_d31_launch(int lc, const TmplArgs& g, long nblk, size_t smem, cudaSt
         return 1;
     }
     if (lc == 1) {
-        k_rys_thread<3, 1, 1, 3, true, true, 1, double><<<dim3((unsigned)nblk, 6), 128, smem, st>>>(g);
+        k_rys_thread<3, 1, 1, 3, true, false, 1, double><<<dim3((unsigned)nblk, 3), 128, smem, st>>>(g);
         return 1;
     }
     if (lc == 2) {
-        k_rys_thread<3, 1, 2, 6, true, true, 1, double><<<dim3((unsigned)nblk, 12), 128, smem, st>>>(g);
+        k_rys_thread<3, 1, 2, 6, true, false, 1, double><<<dim3((unsigned)nblk, 6), 128, smem, st>>>(g);
         return 1;
     }
     if (lc == 3) {
-        k_rys_thread<3, 1, 3, 10, true, true, 1, double><<<dim3((unsigned)nblk, 20), 128, smem, st>>>(g);
+        k_rys_thread<3, 1, 3, 10, true, false, 1, double><<<dim3((unsigned)nblk, 10), 128, smem, st>>>(g);
         return 1;
     }
     if (lc == 4) {
-        k_rys_thread<3, 1, 4, 15, true, true, 1, double><<<dim3((unsigned)nblk, 30), 128, smem, st>>>(g);
+        k_rys_thread<3, 1, 4, 15, true, false, 1, double><<<dim3((unsigned)nblk, 15), 128, smem, st>>>(g);
         return 1;
     }
     if (lc == 5) {
-        k_rys_thread<3, 1, 5, 21, true, true, 1, double><<<dim3((unsigned)nblk, 42), 128, smem, st>>>(g);
+        k_rys_thread<3, 1, 5, 21, true, false, 1, double><<<dim3((unsigned)nblk, 21), 128, smem, st>>>(g);
         return 1;
     }
     return 0;

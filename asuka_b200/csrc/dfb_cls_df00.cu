@@ -28,7 +28,7 @@ int dfb_cls_df00_launch(int lc, const TmplArgs& g, long nblk, size_t smem, cudaS
         return 1;
     }
     if (lc == 6) {
-        k_rys_thread<0, 0, 6, 3, true, false, 1, float><<<dim3((unsigned)nblk, 3), 128, smem, st>>>(g);
+        k_rys_thread<0, 0, 6, 2, true, false, 1, float><<<dim3((unsigned)nblk, 2), 128, smem, st>>>(g);
         return 1;
     }
     return 0;

@@ -12,7 +12,7 @@ int dfb_cls_df11_launch(int lc, const TmplArgs& g, long nblk, size_t smem, cudaS
         return 1;
     }
     if (lc == 2) {
-        k_rys_thread<1, 1, 2, 3, true, false, 1, float><<<dim3((unsigned)nblk, 3), 128, smem, st>>>(g);
+        k_rys_thread<1, 1, 2, 2, true, false, 1, float><<<dim3((unsigned)nblk, 2), 128, smem, st>>>(g);
         return 1;
     }
     if (lc == 3) {

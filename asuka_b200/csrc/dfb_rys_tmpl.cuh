@@ -237,15 +237,19 @@ struct Cls {
     static constexpr int NL = F1 - F0;
     static constexpr int NA = c_ncart(LA), NB = c_ncart(LB);
     static constexpr int NARR = MODE == 0 ? 1 : (MODE == 1 ? 3 : 2);
+    // Angular range [lo(k), hi(k)] of the contracted intermediate accumulated in array k: only
+    // what the epilogue reads.  Derivative (MODE 1, both centres): array 0 (weight 1) feeds the
+    // (a-1, b) and (a, b-1) terms, array 1 (weight 2a) the (a+1, b) term, array 2 (weight 2b) the
+    // (a, b+1) = (a+1, b) + AB (a, b) term.  MODE 2 / 3: the centre-A / centre-B halves.
     __host__ __device__ static constexpr int lo(int k) {
         return MODE == 0 ? LA
-             : MODE == 1 ? (LA > 0 ? LA - 1 : 0)
+             : MODE == 1 ? (k == 0 ? (LA > 0 ? LA - 1 : 0) : (k == 1 ? LA + 1 : LA))
              : MODE == 2 ? (k == 0 ? (LA > 0 ? LA - 1 : 0) : LA + 1)
                          : LA;
     }
     __host__ __device__ static constexpr int hi(int k) {
         return MODE == 0 ? LA + LB
-             : MODE == 1 ? NM
+             : MODE == 1 ? (k == 0 ? LA + LB - 1 : NM)
              : MODE == 2 ? (k == 0 ? (LA > 0 ? LA + LB - 1 : -1) : LA + LB + 1)
                          : (k == 0 ? LA + LB - 1 : LA + LB + 1);
     }

@@ -19,7 +19,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LA_MAX = 3   # AO shells up to f
 LC_MAX = 6   # aux shells up to i
 FS_MAX = 28
-ACC_BUDGET = {False: 40, True: 66}   # doubles of accumulators per thread
+ACC_BUDGET = {False: 40, True: 40}   # doubles of live accumulators per thread
 G_BUDGET = 48                          # doubles of the three 2D recurrence tables (column-limited)
 
 
@@ -54,7 +54,7 @@ def acc_per_f(la, lb, mode):
     if mode == 0:
         return nrange(la, la + lb)
     if mode == 1:
-        return 3 * nrange(max(la - 1, 0), la + lb + 1)
+        return nrange(max(la - 1, 0), la + lb - 1) + nrange(la + 1, la + lb + 1) + nrange(la, la + lb + 1)
     if mode == 2:
         return (nrange(la - 1, la + lb - 1) if la > 0 else 0) + nrange(la + 1, la + lb + 1)
     return nrange(la, la + lb - 1) + nrange(la, la + lb + 1)
@@ -67,24 +67,34 @@ def _key(la, lb, lc, deriv):
 def plan(la, lb, lc, deriv, budget=None, f32=False):
     """(FS, SPLIT) for a class, or None when it stays on the generic warp kernel.
 
-    ``budget`` overrides the accumulator budget; without it the measured per-class table
-    (``class_tuning.json``, "acc_budget") or the default ACC_BUDGET applies.  The
-    environment variable DFB_GEN_ACC_BUDGET_DERIV sets the derivative default (the tuner's
-    variant builds) and DFB_GEN_ACC_BUDGET_INT the integral one.  Budgets count doubles;
-    the mixed-precision kernels (``f32``) hold float accumulators and recurrence tables, so
-    the same registers hold twice as many elements.
+    ``budget`` overrides the accumulator budget.  Otherwise, for the FP64 kernels, the
+    environment variable DFB_GEN_ACC_BUDGET_DERIV (derivative classes) or
+    DFB_GEN_ACC_BUDGET_INT (integral classes) sets the budget of every class of that kind (the
+    tuner's variant builds), else the measured per-class table (``class_tuning.json``,
+    "acc_budget"), else ACC_BUDGET.  Budgets count the live accumulators (the ones the
+    epilogue reads) in doubles.  The mixed-precision kernels (``f32``) hold float accumulators
+    and recurrence tables, so the same registers hold twice as many elements; their budget
+    counts floats: DFB_GEN_ACC_BUDGET_DERIV_F32 / DFB_GEN_ACC_BUDGET_INT_F32 (variant builds),
+    else the table's "acc_budget_f32", else twice the FP64 class's budget.
     """
+    gbudget = 2 * G_BUDGET if f32 else G_BUDGET
     if budget is None:
-        budget = tuning("acc_budget").get(_key(la, lb, lc, deriv))
-    if budget is None:
-        env = os.environ.get("DFB_GEN_ACC_BUDGET_DERIV" if deriv else "DFB_GEN_ACC_BUDGET_INT")
-        budget = int(env) if env else ACC_BUDGET[deriv]
-    gbudget = G_BUDGET
-    if f32:
-        budget, gbudget = 2 * budget, 2 * G_BUDGET
+        kind = "DERIV" if deriv else "INT"
+        env = os.environ.get(f"DFB_GEN_ACC_BUDGET_{kind}_F32" if f32 else f"DFB_GEN_ACC_BUDGET_{kind}")
+        if env:
+            budget = int(env)
+        elif f32 and _key(la, lb, lc, deriv) in tuning("acc_budget_f32"):
+            budget = tuning("acc_budget_f32")[_key(la, lb, lc, deriv)]
+        else:
+            budget = tuning("acc_budget").get(_key(la, lb, lc, deriv), ACC_BUDGET[deriv])
+            if f32:
+                budget *= 2
+    elif f32:
+        budget *= 2
     nm = la + lb + (1 if deriv else 0)
     nf = ncart(lc)
     modes = [(1, False), (None, True)] if deriv else [(0, False)]
+    best = None
     for mode, split in modes:
         per_f = max(acc_per_f(la, lb, 2), acc_per_f(la, lb, 3)) if split else acc_per_f(la, lb, mode)
         for fs in range(1, min(nf, FS_MAX) + 1):
@@ -92,14 +102,19 @@ def plan(la, lb, lc, deriv, budget=None, f32=False):
             if -(-nf // nfs) != fs:
                 continue  # keep the split exact (no empty subsets)
             if per_f * nfs <= budget and g_cost(nm, lc, nfs) <= gbudget:
-                return fs, split
-    return None
+                # each pass repeats the task's roots and recurrence tables: fewest passes wins,
+                # the unsplit form on a tie
+                passes = fs * (2 if split else 1)
+                if best is None or passes < best[0]:
+                    best = (passes, fs, split)
+                break
+    return None if best is None else (best[1], best[2])
 
 
 def tuning(field: str = "min_blocks") -> dict:
     """Per-class choices measured by asuka_b200.tune_classes ("min_blocks": launch bounds,
     "acc_budget": accumulator budget of the component split); empty when absent or when
-    DFB_GEN_NO_TUNING is set (the tuner's variant builds)."""
+    DFB_GEN_NO_TUNING is set (a build with every class at the default shape)."""
     import json
 
     p = os.path.join(HERE, "class_tuning.json")
@@ -124,12 +139,24 @@ def _groups():
     return out
 
 
+def _write(name: str, text: str) -> None:
+    """Write a generated file only when its content changes (keeps the build incremental)."""
+    path = os.path.join(HERE, name)
+    if os.path.exists(path):
+        with open(path) as f:
+            if f.read() == text:
+                return
+    with open(path, "w") as f:
+        f.write(text)
+
+
 def main() -> None:
     tune = tuning()
-    for old in os.listdir(HERE):
-        if old.startswith("dfb_cls_") and old.endswith(".cu"):
-            os.remove(os.path.join(HERE, old))
     groups = _groups()
+    keep = {name + ".cu" for name, *_ in groups}
+    for old in os.listdir(HERE):
+        if old.startswith("dfb_cls_") and old.endswith(".cu") and old not in keep:
+            os.remove(os.path.join(HERE, old))
     for name, deriv, f32, la, lb, cls in groups:
         lines = [
             "// Generated by gen_classes.py -- class-specialised Rys kernel instantiations.",
@@ -147,8 +174,7 @@ def main() -> None:
             lines.append("        return 1;")
             lines.append("    }")
         lines += ["    return 0;", "}", "}  // namespace dfb", ""]
-        with open(os.path.join(HERE, name + ".cu"), "w") as f:
-            f.write("\n".join(lines))
+        _write(name + ".cu", "\n".join(lines))
     # dispatcher header
     hdr = ["// Generated by gen_classes.py -- dispatch over the class-specialised kernels.", "#pragma once",
            '#include "dfb_rys_tmpl.cuh"', "", "namespace dfb {"]
@@ -174,8 +200,7 @@ def main() -> None:
             "    for (int i = 0; i < n; ++i)",
             "        if (k[i][0] == la && k[i][1] == lb && k[i][2] == lc) return true;",
             "    return false;", "}", "}  // namespace dfb", ""]
-    with open(os.path.join(HERE, "dfb_cls_dispatch.h"), "w") as f:
-        f.write("\n".join(hdr))
+    _write("dfb_cls_dispatch.h", "\n".join(hdr))
     print("generated", len(groups), "groups")
 
 

@@ -29,6 +29,7 @@ from __future__ import annotations
 import numpy as np
 import torch
 
+from . import _lib
 from . import linalg as _la
 from . import mixed as _mixed
 from . import tc as _tc
@@ -62,6 +63,27 @@ def _jk_streams(device: torch.device):
     if idx not in _JK_STREAMS:
         _JK_STREAMS[idx] = (torch.cuda.Stream(device=device), torch.cuda.Stream(device=device))
     return _JK_STREAMS[idx]
+
+
+def _gamma_into(Cw: torch.Tensor, A: torch.Tensor, out: torch.Tensor) -> torch.Tensor:
+    """out[P] = Cw A_P Cw^T for symmetric A_P ((nP, nocc, nocc); out (nP, nao, nao), contiguous).
+
+    U = Cw [A_0 | A_1 | ...] as one GEMM ((nao, nP nocc)), then the library's symmetric FP64
+    kernel (``dfb_gamma_sym``: upper tiles only, each written with its transpose): the inner
+    dimension is only nocc, so the product is bound by writing Gamma, and cuBLAS ran it at about
+    half the FP64 rate."""
+    nP, nocc = A.shape[0], A.shape[1]
+    nao = Cw.shape[0]
+    if nP == 0:
+        return out
+    Cw = Cw.contiguous()
+    U = Cw @ A.permute(1, 0, 2).reshape(nocc, nP * nocc)  # (nao, nP, nocc): U[mu, P, j] = (Cw A_P)[mu, j]
+    if not out.is_contiguous():
+        raise ValueError("Gamma output must be contiguous")
+    rc = _lib.lib().dfb_gamma_sym(nP, nao, nocc, _lib.ptr(U), nP * nocc, nocc, _lib.ptr(Cw), _lib.ptr(out),
+                                  int(torch.cuda.current_stream(out.device).cuda_stream))
+    _lib.check(rc, "dfb_gamma_sym")
+    return out
 
 
 def _fork(main: torch.cuda.Stream, side: torch.cuda.Stream) -> None:
@@ -154,12 +176,11 @@ def df_adjoints(engine: DFEngine, Cw: torch.Tensor, saved: dict, precision: str 
     # Gamma_P = d_P D - 1/2 Cw Z_P Cw^T = Cw (d_P I - 1/2 Z_P) Cw^T since D = Cw Cw^T:
     # one batched GEMM, written over X's storage (X is not needed afterwards)
     Zp = -0.5 * Zq + d.view(naux, 1, 1) * torch.eye(nocc, dtype=Zq.dtype, device=Zq.device)
-    T = torch.matmul(Zp, Cw.T)  # (naux, nocc, nao)
     G3 = X
     if precision != "fp64" and MIXED_GAMMA_TC:
-        _tc.bmm(Cw, T, out=G3)
+        _tc.bmm(Cw, torch.matmul(Zp, Cw.T), out=G3)
     else:
-        torch.matmul(Cw, T, out=G3)
+        _gamma_into(Cw, Zp, G3)
     G2 = -0.5 * torch.outer(d, d) + 0.25 * (Z @ Z.T)
     return G3, G2
 
@@ -288,9 +309,8 @@ def df_energy_grad_streamed(engine: DFEngine, Cw: torch.Tensor, aux_block: int =
     ev[3].record()
     for p0, p1, blk in blocks:
         Zp = -0.5 * Zq[p0:p1] + d[p0:p1].view(-1, 1, 1) * eye
-        T = torch.matmul(Zp, Cw.T)
         G3 = Xb_buf[: p1 - p0]
-        torch.matmul(Cw, T, out=G3)
+        _gamma_into(Cw, Zp, G3)
         engine.deriv3c_block(blk, G3, grad, precision=precision)
     ev[4].record()
     G2 = -0.5 * torch.outer(d, d) + 0.25 * (Z @ Z.T)

@@ -19,7 +19,10 @@ NB = 256  # rows per diagonal block
 
 
 def diag_block_inverses(L: torch.Tensor, nb: int = NB) -> list[torch.Tensor]:
-    """Inverses of the nb x nb diagonal blocks of the lower-triangular L."""
+    """Inverses of the nb x nb diagonal blocks of the lower-triangular L.
+
+    About 1 ms for eight 256-row blocks on a B200, whether per block, batched, or read off one
+    solve of the whole L against the identity (measured); the per-block form is kept."""
     n = L.shape[0]
     out = []
     for r0 in range(0, n, nb):

@@ -172,6 +172,16 @@ int dfb_tc_gemm(long M, long N, long K, long batch, const dfb_tc_operand_t *A, c
  * last reset (0 = none; 1, 2 = an mbarrier wait gave up).  Synchronous. */
 int dfb_tc_error(int reset);
 
+/*
+ * 3c adjoint of the DF gradient: out[P] = U_P Cw^T for P < nP, written (nP, nao, nao)
+ * contiguous and exactly symmetric, where U_P = Cw A_P with A_P symmetric (so U_P Cw^T =
+ * Cw A_P Cw^T).  U element (P, mu, j) at U[mu * sU_mu + P * sU_P + j], j < nocc; Cw is
+ * (nao, nocc) contiguous.  FP64.  Replaces the adjoint GEMMs of the whitened-factor route
+ * (asuka/integrals/df_adjoint.py:172-235); no counterpart of its own in the reference.
+ */
+int dfb_gamma_sym(long nP, int nao, int nocc, const double *U, long sU_mu, long sU_P, const double *Cw,
+                  double *out, void *stream);
+
 /* Scratch doubles dfb_rys_int / dfb_rys_deriv need for this class and task count. */
 long dfb_rys_scratch_doubles(int la, int lb, int lc, long ntask, int deriv);
 

@@ -56,6 +56,22 @@ def test_tensor_core_gemm_rejects_bad_arguments_without_a_gpu():
     assert L.dfb_tc_gemm(0, 8, 4, 1, ctypes.byref(a), ctypes.byref(b), 0x3000, 8, 0, 1, 0, 3, 0, None) == 0
 
 
+def test_gamma_kernel_rejects_bad_arguments_without_a_gpu():
+    """Argument checks of dfb_gamma_sym run before any device call; empty shapes are a no-op."""
+    from asuka_b200 import _lib
+
+    L = _lib.lib()
+    cases = [((-1, 8, 4, 0x1000, 32, 4, 0x2000, 0x3000), "invalid sizes"),
+             ((2, 8, 0, 0x1000, 32, 4, 0x2000, 0x3000), "nocc == 0"),
+             ((2, 8, 4, 0, 32, 4, 0x2000, 0x3000), "invalid pointers"),
+             ((2, 8, 4, 0x1000, 3, 4, 0x2000, 0x3000), "invalid pointers or strides")]
+    for args, msg in cases:
+        assert L.dfb_gamma_sym(*args, None) == -1, args
+        assert msg in L.dfb_last_error().decode(), (args, L.dfb_last_error())
+    assert L.dfb_gamma_sym(0, 8, 4, 0, 0, 0, 0, 0, None) == 0
+    assert L.dfb_gamma_sym(3, 0, 4, 0, 0, 0, 0, 0, None) == 0
+
+
 def test_precision_entry_points_reject_unknown_precision_without_a_gpu():
     import ctypes
 

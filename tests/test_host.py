@@ -131,15 +131,20 @@ def test_class_planner_budget_and_table(tmp_path, monkeypatch):
     gc = importlib.util.module_from_spec(spec)
     spec.loader.exec_module(gc)
     gc.HERE = str(tmp_path)
-    fs66, _ = gc.plan(1, 0, 4, True, budget=66)
-    fs100, _ = gc.plan(1, 0, 4, True, budget=100)
-    assert fs100 < fs66
-    (tmp_path / "class_tuning.json").write_text(json.dumps({"min_blocks": {"d104": 4}, "acc_budget": {"d104": 100}}))
+    fs40, _ = gc.plan(1, 0, 4, True, budget=40)
+    fs96, _ = gc.plan(1, 0, 4, True, budget=96)
+    assert fs96 < fs40
+    # live accumulators of the derivative form: (a-1)..(a+b-1), (a+1)..(a+b+1), a..(a+b+1)
+    assert gc.acc_per_f(1, 0, 1) == 1 + 6 + 9 and gc.acc_per_f(0, 0, 1) == 0 + 3 + 4
+    (tmp_path / "class_tuning.json").write_text(json.dumps({"min_blocks": {"d104": 4}, "acc_budget": {"d104": 96}}))
     assert gc.tuning()["d104"] == 4
-    assert gc.plan(1, 0, 4, True) == gc.plan(1, 0, 4, True, budget=100)
+    assert gc.plan(1, 0, 4, True) == gc.plan(1, 0, 4, True, budget=96)
+    monkeypatch.setenv("DFB_GEN_ACC_BUDGET_DERIV", "56")  # a variant build: every derivative class
+    assert gc.plan(1, 0, 4, True) == gc.plan(1, 0, 4, True, budget=56)
+    monkeypatch.delenv("DFB_GEN_ACC_BUDGET_DERIV")
     monkeypatch.setenv("DFB_GEN_NO_TUNING", "1")
     assert gc.tuning() == {}
-    assert gc.plan(1, 0, 4, True) == gc.plan(1, 0, 4, True, budget=66)
+    assert gc.plan(1, 0, 4, True) == gc.plan(1, 0, 4, True, budget=gc.ACC_BUDGET[True])
 
 
 def test_overlap_gradient_contraction_matches_reference():
