@@ -18,18 +18,48 @@ import torch
 NB = 256  # rows per diagonal block
 
 
+INV_BASE = 64  # rows of the diagonal sub-blocks inverted by triangular solves
+
+
 def diag_block_inverses(L: torch.Tensor, nb: int = NB) -> list[torch.Tensor]:
     """Inverses of the nb x nb diagonal blocks of the lower-triangular L.
 
-    About 1 ms for eight 256-row blocks on a B200, whether per block, batched, or read off one
-    solve of the whole L against the identity (measured); the per-block form is kept."""
+    Triangular solves against the identity cost about 0.13 ms per 256-row block on a B200
+    whatever their batching, so only the 64-row sub-blocks are inverted that way (one batched
+    call); the larger inverses are assembled level by level with batched GEMMs,
+    inv([[A, 0], [B, C]]) = [[A^-1, 0], [-C^-1 B A^-1, C^-1]] (0.27 against 1.0 ms for eight
+    256-row blocks).  L is padded to whole blocks with the identity."""
     n = L.shape[0]
-    out = []
-    for r0 in range(0, n, nb):
-        r1 = min(n, r0 + nb)
-        eye = torch.eye(r1 - r0, dtype=L.dtype, device=L.device)
-        out.append(torch.linalg.solve_triangular(L[r0:r1, r0:r1], eye, upper=False))
-    return out
+    base = INV_BASE
+    if nb % base or (nb // base) & (nb // base - 1):  # nb must be base * 2^k
+        out = []
+        for r0 in range(0, n, nb):
+            r1 = min(n, r0 + nb)
+            eye = torch.eye(r1 - r0, dtype=L.dtype, device=L.device)
+            out.append(torch.linalg.solve_triangular(L[r0:r1, r0:r1], eye, upper=False))
+        return out
+    nbk = (n + nb - 1) // nb
+    N = nbk * nb
+    Lp = torch.eye(N, dtype=L.dtype, device=L.device)
+    Lp[:n, :n] = L
+    D = Lp.view(nbk, nb, nbk, nb).diagonal(dim1=0, dim2=2).permute(2, 0, 1)  # (nbk, nb, nb) diagonal blocks
+    m = nb // base
+    sub = D.reshape(nbk, m, base, m, base).diagonal(dim1=1, dim2=3).permute(0, 3, 1, 2).reshape(nbk * m, base, base)
+    eye = torch.eye(base, dtype=L.dtype, device=L.device).expand(nbk * m, base, base)
+    inv = torch.linalg.solve_triangular(sub, eye, upper=False)
+    s = base
+    while s < nb:  # blocks of 2s from the inverses of their two diagonal s-blocks
+        q = nb // (2 * s)
+        pair = inv.view(nbk, q, 2, s, s)
+        Ai, Ci = pair[:, :, 0], pair[:, :, 1]
+        big = D.reshape(nbk, q, 2 * s, q, 2 * s).diagonal(dim1=1, dim2=3).permute(0, 3, 1, 2)
+        nxt = torch.zeros((nbk, q, 2 * s, 2 * s), dtype=L.dtype, device=L.device)
+        nxt[:, :, :s, :s] = Ai
+        nxt[:, :, s:, s:] = Ci
+        nxt[:, :, s:, :s] = -(Ci @ (big[:, :, s:, :s] @ Ai))
+        inv = nxt.reshape(nbk * q, 2 * s, 2 * s)
+        s *= 2
+    return [inv[i, : min(n, r0 + nb) - r0, : min(n, r0 + nb) - r0] for i, r0 in enumerate(range(0, n, nb))]
 
 
 def solve_lower(L: torch.Tensor, Y: torch.Tensor, inv: list[torch.Tensor] | None = None, nb: int = NB,

@@ -88,6 +88,14 @@ def test_block_substitution_matches_triangular_solve():
     Y = torch.randn(n, 37, generator=g, dtype=torch.float64)
     ref = torch.linalg.solve_triangular(L, Y, upper=False)
     inv = linalg.diag_block_inverses(L)
+    # the inverses assembled from 64-row sub-blocks, and the per-block form (a block size that is
+    # not 64 * 2^k), against dense inverses
+    for nb, blocks in ((linalg.NB, inv), (100, linalg.diag_block_inverses(L, 100))):
+        for i, r0 in enumerate(range(0, n, nb)):
+            r1 = min(n, r0 + nb)
+            dense = torch.linalg.inv(L[r0:r1, r0:r1])
+            assert blocks[i].shape == dense.shape
+            assert float((blocks[i] - dense).abs().max()) <= 1e-12 * float(dense.abs().max())
     assert torch.allclose(linalg.solve_lower(L, Y, inv), ref, rtol=0, atol=1e-12 * float(ref.abs().max()))
     Yc = Y.clone()
     linalg.solve_lower(L, Yc, inv, out=Yc)  # in place
