@@ -16,7 +16,7 @@ int dfb_cls_df11_launch(int lc, const TmplArgs& g, long nblk, size_t smem, cudaS
         return 1;
     }
     if (lc == 3) {
-        k_rys_thread<1, 1, 3, 3, true, false, 1, float><<<dim3((unsigned)nblk, 3), 128, smem, st>>>(g);
+        k_rys_thread<1, 1, 3, 4, true, false, 1, float><<<dim3((unsigned)nblk, 4), 128, smem, st>>>(g);
         return 1;
     }
     if (lc == 4) {

@@ -16,7 +16,7 @@ int dfb_cls_df20_launch(int lc, const TmplArgs& g, long nblk, size_t smem, cudaS
         return 1;
     }
     if (lc == 3) {
-        k_rys_thread<2, 0, 3, 2, true, false, 1, float><<<dim3((unsigned)nblk, 2), 128, smem, st>>>(g);
+        k_rys_thread<2, 0, 3, 3, true, false, 1, float><<<dim3((unsigned)nblk, 3), 128, smem, st>>>(g);
         return 1;
     }
     if (lc == 4) {
@@ -24,11 +24,11 @@ int dfb_cls_df20_launch(int lc, const TmplArgs& g, long nblk, size_t smem, cudaS
         return 1;
     }
     if (lc == 5) {
-        k_rys_thread<2, 0, 5, 5, true, true, 1, float><<<dim3((unsigned)nblk, 10), 128, smem, st>>>(g);
+        k_rys_thread<2, 0, 5, 6, true, false, 1, float><<<dim3((unsigned)nblk, 6), 128, smem, st>>>(g);
         return 1;
     }
     if (lc == 6) {
-        k_rys_thread<2, 0, 6, 6, true, true, 1, float><<<dim3((unsigned)nblk, 12), 128, smem, st>>>(g);
+        k_rys_thread<2, 0, 6, 7, true, false, 1, float><<<dim3((unsigned)nblk, 7), 128, smem, st>>>(g);
         return 1;
     }
     return 0;

@@ -16,11 +16,11 @@ int dfb_cls_df21_launch(int lc, const TmplArgs& g, long nblk, size_t smem, cudaS
         return 1;
     }
     if (lc == 3) {
-        k_rys_thread<2, 1, 3, 2, true, true, 1, float><<<dim3((unsigned)nblk, 4), 128, smem, st>>>(g);
+        k_rys_thread<2, 1, 3, 5, true, false, 1, float><<<dim3((unsigned)nblk, 5), 128, smem, st>>>(g);
         return 1;
     }
     if (lc == 4) {
-        k_rys_thread<2, 1, 4, 5, true, false, 1, float><<<dim3((unsigned)nblk, 5), 128, smem, st>>>(g);
+        k_rys_thread<2, 1, 4, 8, true, false, 1, float><<<dim3((unsigned)nblk, 8), 128, smem, st>>>(g);
         return 1;
     }
     if (lc == 5) {

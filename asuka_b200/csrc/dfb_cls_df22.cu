@@ -20,15 +20,15 @@ int dfb_cls_df22_launch(int lc, const TmplArgs& g, long nblk, size_t smem, cudaS
         return 1;
     }
     if (lc == 4) {
-        k_rys_thread<2, 2, 4, 8, true, false, 1, float><<<dim3((unsigned)nblk, 8), 128, smem, st>>>(g);
+        k_rys_thread<2, 2, 4, 15, true, false, 1, float><<<dim3((unsigned)nblk, 15), 128, smem, st>>>(g);
         return 1;
     }
     if (lc == 5) {
-        k_rys_thread<2, 2, 5, 11, true, false, 1, float><<<dim3((unsigned)nblk, 11), 128, smem, st>>>(g);
+        k_rys_thread<2, 2, 5, 21, true, false, 1, float><<<dim3((unsigned)nblk, 21), 128, smem, st>>>(g);
         return 1;
     }
     if (lc == 6) {
-        k_rys_thread<2, 2, 6, 28, true, true, 1, float><<<dim3((unsigned)nblk, 56), 128, smem, st>>>(g);
+        k_rys_thread<2, 2, 6, 28, true, false, 1, float><<<dim3((unsigned)nblk, 28), 128, smem, st>>>(g);
         return 1;
     }
     return 0;

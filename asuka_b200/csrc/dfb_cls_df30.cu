@@ -8,7 +8,7 @@ int dfb_cls_df30_launch(int lc, const TmplArgs& g, long nblk, size_t smem, cudaS
         return 1;
     }
     if (lc == 1) {
-        k_rys_thread<3, 0, 1, 1, true, false, 1, float><<<dim3((unsigned)nblk, 1), 128, smem, st>>>(g);
+        k_rys_thread<3, 0, 1, 2, true, false, 1, float><<<dim3((unsigned)nblk, 2), 128, smem, st>>>(g);
         return 1;
     }
     if (lc == 2) {

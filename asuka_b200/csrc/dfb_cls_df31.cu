@@ -8,27 +8,27 @@ int dfb_cls_df31_launch(int lc, const TmplArgs& g, long nblk, size_t smem, cudaS
         return 1;
     }
     if (lc == 1) {
-        k_rys_thread<3, 1, 1, 2, true, false, 1, float><<<dim3((unsigned)nblk, 2), 128, smem, st>>>(g);
+        k_rys_thread<3, 1, 1, 3, true, false, 1, float><<<dim3((unsigned)nblk, 3), 128, smem, st>>>(g);
         return 1;
     }
     if (lc == 2) {
-        k_rys_thread<3, 1, 2, 3, true, false, 1, float><<<dim3((unsigned)nblk, 3), 128, smem, st>>>(g);
+        k_rys_thread<3, 1, 2, 6, true, false, 1, float><<<dim3((unsigned)nblk, 6), 128, smem, st>>>(g);
         return 1;
     }
     if (lc == 3) {
-        k_rys_thread<3, 1, 3, 5, true, false, 1, float><<<dim3((unsigned)nblk, 5), 128, smem, st>>>(g);
+        k_rys_thread<3, 1, 3, 10, true, false, 1, float><<<dim3((unsigned)nblk, 10), 128, smem, st>>>(g);
         return 1;
     }
     if (lc == 4) {
-        k_rys_thread<3, 1, 4, 8, true, false, 1, float><<<dim3((unsigned)nblk, 8), 128, smem, st>>>(g);
+        k_rys_thread<3, 1, 4, 15, true, false, 1, float><<<dim3((unsigned)nblk, 15), 128, smem, st>>>(g);
         return 1;
     }
     if (lc == 5) {
-        k_rys_thread<3, 1, 5, 11, true, false, 1, float><<<dim3((unsigned)nblk, 11), 128, smem, st>>>(g);
+        k_rys_thread<3, 1, 5, 21, true, false, 1, float><<<dim3((unsigned)nblk, 21), 128, smem, st>>>(g);
         return 1;
     }
     if (lc == 6) {
-        k_rys_thread<3, 1, 6, 28, true, true, 1, float><<<dim3((unsigned)nblk, 56), 128, smem, st>>>(g);
+        k_rys_thread<3, 1, 6, 28, true, false, 1, float><<<dim3((unsigned)nblk, 28), 128, smem, st>>>(g);
         return 1;
     }
     return 0;

@@ -12,7 +12,7 @@ int dfb_cls_i30_launch(int lc, const TmplArgs& g, long nblk, size_t smem, cudaSt
         return 1;
     }
     if (lc == 2) {
-        k_rys_thread<3, 0, 2, 2, false, false, 1, double><<<dim3((unsigned)nblk, 2), 128, smem, st>>>(g);
+        k_rys_thread<3, 0, 2, 2, false, false, 3, double><<<dim3((unsigned)nblk, 2), 128, smem, st>>>(g);
         return 1;
     }
     if (lc == 3) {
