@@ -96,7 +96,8 @@ def flops_3c(ao, aux, deriv: bool = False) -> float:
 
 
 def flops_deriv3c(ao, aux) -> float:
-    """Algorithmic FLOPs of the 3c derivative contraction (per-unit model of the survey, 8(d))."""
+    """Algorithmic FLOPs of the 3c derivative contraction, per primitive triplet
+    K_ab K_P n_r' (25 n_A n_B n_P + 9 (l_a+l_b+2)(l_P+2)) summed over every (AO shell pair, aux shell)."""
     from asuka_b200.basis import build_shell_pairs_l_order, ncart
 
     sp = build_shell_pairs_l_order(ao)
