@@ -57,6 +57,7 @@ _SIGS = {
                                                           ctypes.c_long, ctypes.c_long, ctypes.c_int, ctypes.c_int,
                                                           ctypes.c_int, ctypes.c_long, _d]),
     "dfb_tc_error": (ctypes.c_int, [ctypes.c_int]),
+    "dfb_rys_error": (ctypes.c_int, [ctypes.c_int]),
     "dfb_gamma_sym": (ctypes.c_int, [ctypes.c_long, ctypes.c_int, ctypes.c_int, _d, ctypes.c_long, ctypes.c_long,
                                      _d, _d, _d]),
     "dfb_fp32_fma_probe": (ctypes.c_int, [_d, ctypes.c_int, ctypes.c_int, ctypes.c_int, _d]),

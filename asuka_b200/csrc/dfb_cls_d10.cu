@@ -4,31 +4,31 @@
 namespace dfb {
 int dfb_cls_d10_launch(int lc, const TmplArgs& g, long nblk, size_t smem, cudaStream_t st) {
     if (lc == 0) {
-        k_rys_thread<1, 0, 0, 1, true, false, 1, double><<<dim3((unsigned)nblk, 1), 128, smem, st>>>(g);
+        k_rys_thread<1, 0, 0, 1, true, false, 1, double, false><<<dim3((unsigned)nblk, 1), 128, smem, st>>>(g);
         return 1;
     }
     if (lc == 1) {
-        k_rys_thread<1, 0, 1, 1, true, false, 1, double><<<dim3((unsigned)nblk, 1), 128, smem, st>>>(g);
+        k_rys_thread<1, 0, 1, 1, true, false, 1, double, false><<<dim3((unsigned)nblk, 1), 128, smem, st>>>(g);
         return 1;
     }
     if (lc == 2) {
-        k_rys_thread<1, 0, 2, 2, true, false, 1, double><<<dim3((unsigned)nblk, 2), 128, smem, st>>>(g);
+        k_rys_thread<1, 0, 2, 2, true, false, 1, double, false><<<dim3((unsigned)nblk, 2), 128, smem, st>>>(g);
         return 1;
     }
     if (lc == 3) {
-        k_rys_thread<1, 0, 3, 4, true, false, 1, double><<<dim3((unsigned)nblk, 4), 128, smem, st>>>(g);
+        k_rys_thread<1, 0, 3, 4, true, false, 1, double, false><<<dim3((unsigned)nblk, 4), 128, smem, st>>>(g);
         return 1;
     }
     if (lc == 4) {
-        k_rys_thread<1, 0, 4, 4, true, false, 1, double><<<dim3((unsigned)nblk, 4), 128, smem, st>>>(g);
+        k_rys_thread<1, 0, 4, 4, true, false, 1, double, false><<<dim3((unsigned)nblk, 4), 128, smem, st>>>(g);
         return 1;
     }
     if (lc == 5) {
-        k_rys_thread<1, 0, 5, 6, true, false, 1, double><<<dim3((unsigned)nblk, 6), 128, smem, st>>>(g);
+        k_rys_thread<1, 0, 5, 6, true, false, 1, double, false><<<dim3((unsigned)nblk, 6), 128, smem, st>>>(g);
         return 1;
     }
     if (lc == 6) {
-        k_rys_thread<1, 0, 6, 10, true, false, 1, double><<<dim3((unsigned)nblk, 10), 128, smem, st>>>(g);
+        k_rys_thread<1, 0, 6, 10, true, false, 1, double, false><<<dim3((unsigned)nblk, 10), 128, smem, st>>>(g);
         return 1;
     }
     return 0;

@@ -4,31 +4,31 @@
 namespace dfb {
 int dfb_cls_d11_launch(int lc, const TmplArgs& g, long nblk, size_t smem, cudaStream_t st) {
     if (lc == 0) {
-        k_rys_thread<1, 1, 0, 1, true, false, 1, double><<<dim3((unsigned)nblk, 1), 128, smem, st>>>(g);
+        k_rys_thread<1, 1, 0, 1, true, false, 1, double, false><<<dim3((unsigned)nblk, 1), 128, smem, st>>>(g);
         return 1;
     }
     if (lc == 1) {
-        k_rys_thread<1, 1, 1, 3, true, false, 1, double><<<dim3((unsigned)nblk, 3), 128, smem, st>>>(g);
+        k_rys_thread<1, 1, 1, 3, true, false, 1, double, false><<<dim3((unsigned)nblk, 3), 128, smem, st>>>(g);
         return 1;
     }
     if (lc == 2) {
-        k_rys_thread<1, 1, 2, 3, true, false, 1, double><<<dim3((unsigned)nblk, 3), 128, smem, st>>>(g);
+        k_rys_thread<1, 1, 2, 3, true, false, 1, double, false><<<dim3((unsigned)nblk, 3), 128, smem, st>>>(g);
         return 1;
     }
     if (lc == 3) {
-        k_rys_thread<1, 1, 3, 5, true, false, 1, double><<<dim3((unsigned)nblk, 5), 128, smem, st>>>(g);
+        k_rys_thread<1, 1, 3, 5, true, false, 1, double, false><<<dim3((unsigned)nblk, 5), 128, smem, st>>>(g);
         return 1;
     }
     if (lc == 4) {
-        k_rys_thread<1, 1, 4, 8, true, false, 1, double><<<dim3((unsigned)nblk, 8), 128, smem, st>>>(g);
+        k_rys_thread<1, 1, 4, 8, true, false, 1, double, false><<<dim3((unsigned)nblk, 8), 128, smem, st>>>(g);
         return 1;
     }
     if (lc == 5) {
-        k_rys_thread<1, 1, 5, 21, true, false, 1, double><<<dim3((unsigned)nblk, 21), 128, smem, st>>>(g);
+        k_rys_thread<1, 1, 5, 21, true, false, 1, double, false><<<dim3((unsigned)nblk, 21), 128, smem, st>>>(g);
         return 1;
     }
     if (lc == 6) {
-        k_rys_thread<1, 1, 6, 28, true, false, 1, double><<<dim3((unsigned)nblk, 28), 128, smem, st>>>(g);
+        k_rys_thread<1, 1, 6, 28, true, false, 1, double, false><<<dim3((unsigned)nblk, 28), 128, smem, st>>>(g);
         return 1;
     }
     return 0;

@@ -4,27 +4,27 @@
 namespace dfb {
 int dfb_cls_d22_launch(int lc, const TmplArgs& g, long nblk, size_t smem, cudaStream_t st) {
     if (lc == 0) {
-        k_rys_thread<2, 2, 0, 1, true, true, 1, double><<<dim3((unsigned)nblk, 2), 128, smem, st>>>(g);
+        k_rys_thread<2, 2, 0, 1, true, true, 1, double, false><<<dim3((unsigned)nblk, 2), 128, smem, st>>>(g);
         return 1;
     }
     if (lc == 1) {
-        k_rys_thread<2, 2, 1, 3, true, true, 1, double><<<dim3((unsigned)nblk, 6), 128, smem, st>>>(g);
+        k_rys_thread<2, 2, 1, 3, true, true, 1, double, false><<<dim3((unsigned)nblk, 6), 128, smem, st>>>(g);
         return 1;
     }
     if (lc == 2) {
-        k_rys_thread<2, 2, 2, 6, true, true, 1, double><<<dim3((unsigned)nblk, 12), 128, smem, st>>>(g);
+        k_rys_thread<2, 2, 2, 6, true, true, 1, double, false><<<dim3((unsigned)nblk, 12), 128, smem, st>>>(g);
         return 1;
     }
     if (lc == 3) {
-        k_rys_thread<2, 2, 3, 10, true, true, 1, double><<<dim3((unsigned)nblk, 20), 128, smem, st>>>(g);
+        k_rys_thread<2, 2, 3, 10, true, true, 1, double, false><<<dim3((unsigned)nblk, 20), 128, smem, st>>>(g);
         return 1;
     }
     if (lc == 4) {
-        k_rys_thread<2, 2, 4, 15, true, false, 1, double><<<dim3((unsigned)nblk, 15), 128, smem, st>>>(g);
+        k_rys_thread<2, 2, 4, 15, true, false, 1, double, false><<<dim3((unsigned)nblk, 15), 128, smem, st>>>(g);
         return 1;
     }
     if (lc == 5) {
-        k_rys_thread<2, 2, 5, 21, true, false, 1, double><<<dim3((unsigned)nblk, 21), 128, smem, st>>>(g);
+        k_rys_thread<2, 2, 5, 21, true, false, 1, double, false><<<dim3((unsigned)nblk, 21), 128, smem, st>>>(g);
         return 1;
     }
     return 0;

@@ -4,27 +4,36 @@
 namespace dfb {
 int dfb_cls_d31_launch(int lc, const TmplArgs& g, long nblk, size_t smem, cudaStream_t st) {
     if (lc == 0) {
-        k_rys_thread<3, 1, 0, 1, true, true, 1, double><<<dim3((unsigned)nblk, 2), 128, smem, st>>>(g);
+        const long ng = (long)(smem / sizeof(double)) - 256L * 3;
+        const size_t sm = sizeof(double) * (size_t)(rys_stage_offset(ng, 3) + rys_stage_doubles(g.tab.nint, 3));
+        static size_t attr[64];
+        int dev = 0;
+        cudaGetDevice(&dev);
+        if (sm > attr[dev & 63]) {
+            cudaFuncSetAttribute(k_rys_thread<3, 1, 0, 1, true, true, 1, double, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+            attr[dev & 63] = sm;
+        }
+        k_rys_thread<3, 1, 0, 1, true, true, 1, double, true><<<dim3((unsigned)nblk, 2), 128, sm, st>>>(g);
         return 1;
     }
     if (lc == 1) {
-        k_rys_thread<3, 1, 1, 3, true, false, 1, double><<<dim3((unsigned)nblk, 3), 128, smem, st>>>(g);
+        k_rys_thread<3, 1, 1, 3, true, false, 1, double, false><<<dim3((unsigned)nblk, 3), 128, smem, st>>>(g);
         return 1;
     }
     if (lc == 2) {
-        k_rys_thread<3, 1, 2, 6, true, false, 1, double><<<dim3((unsigned)nblk, 6), 128, smem, st>>>(g);
+        k_rys_thread<3, 1, 2, 6, true, false, 1, double, false><<<dim3((unsigned)nblk, 6), 128, smem, st>>>(g);
         return 1;
     }
     if (lc == 3) {
-        k_rys_thread<3, 1, 3, 10, true, false, 1, double><<<dim3((unsigned)nblk, 10), 128, smem, st>>>(g);
+        k_rys_thread<3, 1, 3, 10, true, false, 1, double, false><<<dim3((unsigned)nblk, 10), 128, smem, st>>>(g);
         return 1;
     }
     if (lc == 4) {
-        k_rys_thread<3, 1, 4, 15, true, false, 1, double><<<dim3((unsigned)nblk, 15), 128, smem, st>>>(g);
+        k_rys_thread<3, 1, 4, 15, true, false, 1, double, false><<<dim3((unsigned)nblk, 15), 128, smem, st>>>(g);
         return 1;
     }
     if (lc == 5) {
-        k_rys_thread<3, 1, 5, 21, true, false, 1, double><<<dim3((unsigned)nblk, 21), 128, smem, st>>>(g);
+        k_rys_thread<3, 1, 5, 21, true, false, 1, double, false><<<dim3((unsigned)nblk, 21), 128, smem, st>>>(g);
         return 1;
     }
     return 0;

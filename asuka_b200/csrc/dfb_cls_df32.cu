@@ -4,31 +4,31 @@
 namespace dfb {
 int dfb_cls_df32_launch(int lc, const TmplArgs& g, long nblk, size_t smem, cudaStream_t st) {
     if (lc == 0) {
-        k_rys_thread<3, 2, 0, 1, true, true, 1, float><<<dim3((unsigned)nblk, 2), 128, smem, st>>>(g);
+        k_rys_thread<3, 2, 0, 1, true, true, 1, float, false><<<dim3((unsigned)nblk, 2), 128, smem, st>>>(g);
         return 1;
     }
     if (lc == 1) {
-        k_rys_thread<3, 2, 1, 3, true, false, 1, float><<<dim3((unsigned)nblk, 3), 128, smem, st>>>(g);
+        k_rys_thread<3, 2, 1, 3, true, false, 1, float, false><<<dim3((unsigned)nblk, 3), 128, smem, st>>>(g);
         return 1;
     }
     if (lc == 2) {
-        k_rys_thread<3, 2, 2, 6, true, false, 1, float><<<dim3((unsigned)nblk, 6), 128, smem, st>>>(g);
+        k_rys_thread<3, 2, 2, 6, true, false, 1, float, false><<<dim3((unsigned)nblk, 6), 128, smem, st>>>(g);
         return 1;
     }
     if (lc == 3) {
-        k_rys_thread<3, 2, 3, 10, true, false, 1, float><<<dim3((unsigned)nblk, 10), 128, smem, st>>>(g);
+        k_rys_thread<3, 2, 3, 10, true, false, 1, float, false><<<dim3((unsigned)nblk, 10), 128, smem, st>>>(g);
         return 1;
     }
     if (lc == 4) {
-        k_rys_thread<3, 2, 4, 15, true, true, 1, float><<<dim3((unsigned)nblk, 30), 128, smem, st>>>(g);
+        k_rys_thread<3, 2, 4, 15, true, true, 1, float, false><<<dim3((unsigned)nblk, 30), 128, smem, st>>>(g);
         return 1;
     }
     if (lc == 5) {
-        k_rys_thread<3, 2, 5, 21, true, true, 1, float><<<dim3((unsigned)nblk, 42), 128, smem, st>>>(g);
+        k_rys_thread<3, 2, 5, 21, true, true, 1, float, false><<<dim3((unsigned)nblk, 42), 128, smem, st>>>(g);
         return 1;
     }
     if (lc == 6) {
-        k_rys_thread<3, 2, 6, 28, true, true, 1, float><<<dim3((unsigned)nblk, 56), 128, smem, st>>>(g);
+        k_rys_thread<3, 2, 6, 28, true, true, 1, float, false><<<dim3((unsigned)nblk, 56), 128, smem, st>>>(g);
         return 1;
     }
     return 0;

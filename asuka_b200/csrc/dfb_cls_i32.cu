@@ -4,23 +4,23 @@
 namespace dfb {
 int dfb_cls_i32_launch(int lc, const TmplArgs& g, long nblk, size_t smem, cudaStream_t st) {
     if (lc == 0) {
-        k_rys_thread<3, 2, 0, 1, false, false, 1, double><<<dim3((unsigned)nblk, 1), 128, smem, st>>>(g);
+        k_rys_thread<3, 2, 0, 1, false, false, 1, double, false><<<dim3((unsigned)nblk, 1), 128, smem, st>>>(g);
         return 1;
     }
     if (lc == 1) {
-        k_rys_thread<3, 2, 1, 3, false, false, 1, double><<<dim3((unsigned)nblk, 3), 128, smem, st>>>(g);
+        k_rys_thread<3, 2, 1, 3, false, false, 1, double, false><<<dim3((unsigned)nblk, 3), 128, smem, st>>>(g);
         return 1;
     }
     if (lc == 2) {
-        k_rys_thread<3, 2, 2, 6, false, false, 1, double><<<dim3((unsigned)nblk, 6), 128, smem, st>>>(g);
+        k_rys_thread<3, 2, 2, 6, false, false, 1, double, false><<<dim3((unsigned)nblk, 6), 128, smem, st>>>(g);
         return 1;
     }
     if (lc == 3) {
-        k_rys_thread<3, 2, 3, 10, false, false, 1, double><<<dim3((unsigned)nblk, 10), 128, smem, st>>>(g);
+        k_rys_thread<3, 2, 3, 10, false, false, 1, double, false><<<dim3((unsigned)nblk, 10), 128, smem, st>>>(g);
         return 1;
     }
     if (lc == 5) {
-        k_rys_thread<3, 2, 5, 21, false, false, 1, double><<<dim3((unsigned)nblk, 21), 128, smem, st>>>(g);
+        k_rys_thread<3, 2, 5, 21, false, false, 1, double, false><<<dim3((unsigned)nblk, 21), 128, smem, st>>>(g);
         return 1;
     }
     return 0;

@@ -30,6 +30,7 @@ struct RysTable {
     int nmax, nint, deg;
     double tmax;
     double inv_h;  // intervals per unit T (nint / tmax)
+    int* err;      // device word: 0, or the code of the first bounded wait that gave up (dfb_rys_error)
 };
 
 // Task t -> (pair list index, aux list index).  grid > 0: pair-major grid with

@@ -565,6 +565,7 @@ struct DeviceTable {
     bool ready = false;
     double* coef = nullptr;
     double* herm = nullptr;
+    int* err = nullptr;  // staging wait error word (RysTable::err)
     RysTable tab;
 };
 static DeviceTable g_tables[64];
@@ -746,11 +747,14 @@ extern "C" int dfb_rys_table_init(const double* coef, const int* offs, long ncoe
     if (t.ready) return DFB_OK;
     cudaError_t e = cudaMalloc(&t.coef, sizeof(double) * ncoef);
     if (e == cudaSuccess) e = cudaMalloc(&t.herm, sizeof(double) * nherm);
+    if (e == cudaSuccess) e = cudaMalloc(&t.err, sizeof(int));
+    if (e == cudaSuccess) e = cudaMemset(t.err, 0, sizeof(int));
     if (e == cudaSuccess) e = cudaMemcpy(t.coef, coef, sizeof(double) * ncoef, cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemcpy(t.herm, herm, sizeof(double) * nherm, cudaMemcpyHostToDevice);
     if (e != cudaSuccess) return set_cuda_error("Rys table upload", e);
     t.tab.coef = t.coef;
     t.tab.herm = t.herm;
+    t.tab.err = t.err;
     for (int n = 0; n <= DFB_NROOTS_MAX; ++n) {
         t.tab.offs[n] = (n >= 1 && n <= nmax) ? offs[n] : 0;
         t.tab.hoff[n] = (n >= 1 && n <= nmax) ? hoffs[n] : 0;
@@ -762,6 +766,18 @@ extern "C" int dfb_rys_table_init(const double* coef, const int* offs, long ncoe
     t.tab.inv_h = (double)nint / tmax;
     t.ready = true;
     return DFB_OK;
+}
+
+extern "C" int dfb_rys_error(int reset) {
+    clear_error();
+    const int dev = current_device();
+    if (dev < 0 || dev >= 64 || !g_tables[dev].ready)
+        return set_error(DFB_ERR_NOT_INITIALISED, "Rys table not uploaded on this device");
+    int v = 0;
+    cudaError_t e = cudaMemcpy(&v, g_tables[dev].err, sizeof(int), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess && reset && v != 0) e = cudaMemset(g_tables[dev].err, 0, sizeof(int));
+    if (e != cudaSuccess) return set_cuda_error("dfb_rys_error", e);
+    return v;
 }
 
 extern "C" int dfb_pair_tables(const double* cxyz, const int* shell_pstart, const int* shell_nprim,

@@ -21,6 +21,7 @@
 //   d/dA = 2a (a+1_d) - a_d (a-1_d),  d/dB = 2b [(a+1_d, b) + AB_d (a, b)] - b_d (a, b-1_d)
 // with the adjoint tile; d/dC = -(d/dA + d/dB) (translational invariance).
 #pragma once
+#include <stdint.h>
 #include <utility>
 
 #include "../../include/dfb_types.h"
@@ -86,8 +87,21 @@ __device__ __forceinline__ double poly9(const double* c, double u, double u2, do
     return fma(p89, u8, fma(q1, u4, q0));
 }
 
-template <int NR>
-__device__ __forceinline__ void rys_eval_t(const RysTable& tab, double T, double (&x)[NR], double (&w)[NR]) {
+// Coefficient pair d of table function r for the row of interval k: global memory through the
+// read-only cache, or the block's shared-memory copy of this root count's table (STAGED).
+template <int NR, bool STAGED>
+__device__ __forceinline__ double2 rys_coef2(const double* cnr, int k, int r, int d) {
+    const double2* c = reinterpret_cast<const double2*>(cnr + (size_t)k * (2 * NR) * (DFB_RYS_DEG + 1)) +
+                       r * ((DFB_RYS_DEG + 1) / 2) + d;
+    if constexpr (STAGED)
+        return *c;
+    else
+        return __ldg(c);
+}
+
+template <int NR, bool STAGED = false>
+__device__ __forceinline__ void rys_eval_t(const RysTable& tab, const double* cnr, double T, double (&x)[NR],
+                                           double (&w)[NR]) {
     if (T >= tab.tmax) {
         const double* h = tab.herm + tab.hoff[NR];
         const double rs = rsqrt(T);
@@ -106,13 +120,12 @@ __device__ __forceinline__ void rys_eval_t(const RysTable& tab, double T, double
     constexpr int S = DFB_RYS_DEG + 1;
     static_assert(S == 10, "poly9 evaluates degree-9 tables");
     const double u2 = u * u, u4 = u2 * u2, u8 = u4 * u4;
-    const double2* c = reinterpret_cast<const double2*>(tab.coef + tab.offs[NR] + (size_t)k * (2 * NR) * S);
 #pragma unroll
     for (int r = 0; r < 2 * NR; ++r) {
         double cf[S];
 #pragma unroll
         for (int d = 0; d < S / 2; ++d) {
-            const double2 v = __ldg(c + r * (S / 2) + d);
+            const double2 v = rys_coef2<NR, STAGED>(cnr, k, r, d);
             cf[2 * d] = v.x;
             cf[2 * d + 1] = v.y;
         }
@@ -128,8 +141,9 @@ __device__ __forceinline__ void rys_eval_t(const RysTable& tab, double T, double
 // shared-memory slot r[0..NR) = nodes, r[NR..2NR) = weights (bounds the
 // coefficient registers in flight); entry i sits at r[i * RS], so the slots of
 // consecutive threads interleave and a warp's stores hit consecutive words.
-template <int NR, int RS>
-__device__ __forceinline__ void rys_eval_smem(const RysTable& tab, double T, double* __restrict__ r) {
+template <int NR, int RS, bool STAGED = false>
+__device__ __forceinline__ void rys_eval_smem(const RysTable& tab, const double* cnr, double T,
+                                              double* __restrict__ r) {
     if (T >= tab.tmax) {
         const double* h = tab.herm + tab.hoff[NR];
         const double rs = rsqrt(T);
@@ -147,14 +161,13 @@ __device__ __forceinline__ void rys_eval_smem(const RysTable& tab, double T, dou
     const double u = 2.0 * (Th - (double)k) - 1.0;
     constexpr int S = DFB_RYS_DEG + 1;
     const double u2 = u * u, u4 = u2 * u2, u8 = u4 * u4;
-    const double2* c = reinterpret_cast<const double2*>(tab.coef + tab.offs[NR] + (size_t)k * (2 * NR) * S);
 #pragma unroll 1
     for (int f = 0; f < 2 * NR; f += 2) {
         double cf0[S], cf1[S];
 #pragma unroll
         for (int d = 0; d < S / 2; ++d) {
-            const double2 v0 = __ldg(c + f * (S / 2) + d);
-            const double2 v1 = __ldg(c + (f + 1) * (S / 2) + d);
+            const double2 v0 = rys_coef2<NR, STAGED>(cnr, k, f, d);
+            const double2 v1 = rys_coef2<NR, STAGED>(cnr, k, f + 1, d);
             cf0[2 * d] = v0.x;
             cf0[2 * d + 1] = v0.y;
             cf1[2 * d] = v1.x;
@@ -426,8 +439,8 @@ struct Cls {
     }
 };
 
-template <class CL>
-__device__ __forceinline__ void rys_thread_body(const TmplArgs& g, long task, double* sgrad) {
+template <class CL, bool STAGED = false>
+__device__ __forceinline__ void rys_thread_body(const TmplArgs& g, long task, double* sgrad, const double* cnr) {
     using R = typename CL::R;
     constexpr int NR = CL::NR, NM = CL::NM, LB = CL::LB;
     // per-thread root slot after the optional gradient buffer
@@ -486,9 +499,9 @@ __device__ __forceinline__ void rys_thread_body(const TmplArgs& g, long task, do
             constexpr int NRR = NR <= 2 ? NR : 1;
             double xr[NRR], wr[NRR];
             if constexpr (NR <= 2)
-                rys_eval_t<NR>(g.tab, T, xr, wr);
+                rys_eval_t<NR, STAGED>(g.tab, cnr, T, xr, wr);
             else
-                rys_eval_smem<NR, RS>(g.tab, T, sroot);
+                rys_eval_smem<NR, RS, STAGED>(g.tab, cnr, T, sroot);
             const double qi = q * inv, pi = p * inv;
             const double h_q = 0.5 * rq;
 #pragma unroll
@@ -568,12 +581,79 @@ __device__ __forceinline__ void rys_thread_body(const TmplArgs& g, long task, do
 #ifndef DFB_THREAD_MIN_BLOCKS
 #define DFB_THREAD_MIN_BLOCKS 1
 #endif
-template <int LA, int LB, int LC, int FS, bool DERIV, bool SPLIT, int MINB = 1, typename R = double>
+
+// Staging of the Rys coefficient table (STAGE): at block start one thread copies this root count's
+// table (nint x 2 NR x 10 doubles: 30 KB per root) from global into shared memory with one bulk
+// asynchronous copy (cp.async.bulk, completion counted on an mbarrier); the block's root
+// evaluations then gather from shared memory instead of L1/L2.  Every wait on the mbarrier is
+// bounded: a block whose wait gives up records an error code (dfb_rys_error), evaluates from the
+// global table, and before it exits waits (bounded) once more for its copy in flight.
+constexpr long RYS_WAIT_LIMIT = 1L << 22;
+
+__device__ __forceinline__ uint32_t rys_smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ bool rys_mbar_wait(uint32_t bar, uint32_t parity) {
+    for (long it = 0; it < RYS_WAIT_LIMIT; ++it) {
+        uint32_t ok;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.b32 %0, 1, 0, p;\n\t}"
+            : "=r"(ok)
+            : "r"(bar), "r"(parity)
+            : "memory");
+        if (ok) return true;
+    }
+    return false;
+}
+
+// Doubles of the shared-memory table copy of root count nr, and its offset after the gradient
+// buffer (ng doubles) and the root slots (128 x 2 nr doubles), rounded to 16 bytes.
+__host__ __device__ constexpr long rys_stage_doubles(int nint, int nr) { return (long)nint * 2 * nr * (DFB_RYS_DEG + 1); }
+__host__ __device__ constexpr long rys_stage_offset(long ng, int nr) { return (ng + 256L * nr + 1) & ~1L; }
+
+template <int LA, int LB, int LC, int FS, bool DERIV, bool SPLIT, int MINB = 1, typename R = double,
+          bool STAGE = false>
 __global__ void __launch_bounds__(128, (DFB_THREAD_MIN_BLOCKS > MINB ? DFB_THREAD_MIN_BLOCKS : MINB))
     k_rys_thread(TmplArgs g) {
     extern __shared__ double sgrad[];
     const int ng = (DERIV && g.smem_grad) ? g.natm * 3 : 0;
-    if (DERIV && g.smem_grad) {
+    constexpr int NR = (LA + LB + LC + (DERIV ? 1 : 0)) / 2 + 1;
+    const double* cnr = g.tab.coef + g.tab.offs[NR];
+    [[maybe_unused]] bool staged = false;
+    [[maybe_unused]] uint32_t bar = 0;
+    if constexpr (STAGE) {
+        __shared__ __align__(8) unsigned long long s_mbar;
+        double* stab = sgrad + rys_stage_offset(ng, NR);
+        const uint32_t bytes = (uint32_t)(rys_stage_doubles(g.tab.nint, NR) * sizeof(double));
+        bar = rys_smem_u32(&s_mbar);
+        staged = ((rys_smem_u32(stab) | (uint32_t)(uintptr_t)cnr) & 15u) == 0;  // uniform over the block
+        if (staged) {
+            if (threadIdx.x == 0) {
+                asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
+                asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+            }
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+                asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
+                                 "r"(rys_smem_u32(stab)), "l"(cnr), "r"(bytes), "r"(bar)
+                             : "memory");
+            }
+        }
+        if (DERIV && g.smem_grad) {
+            for (int i = threadIdx.x; i < ng; i += blockDim.x) sgrad[i] = 0.0;
+        }
+        if (staged) {
+            if (rys_mbar_wait(bar, 0)) {
+                cnr = stab;
+            } else {
+                atomicCAS(g.tab.err, 0, 1);
+                staged = false;  // evaluate from the global table; the copy is waited for at exit
+            }
+        }
+        __syncthreads();
+    } else if (DERIV && g.smem_grad) {
         for (int i = threadIdx.x; i < ng; i += blockDim.x) sgrad[i] = 0.0;
         __syncthreads();
     }
@@ -584,9 +664,10 @@ __global__ void __launch_bounds__(128, (DFB_THREAD_MIN_BLOCKS > MINB ? DFB_THREA
 #define DFB_FSI(I)                                                                                              \
     case I:                                                                                                     \
         if constexpr (I < FS)                                                                                   \
-            rys_thread_body<Cls<LA, LB, LC, FS, (I < FS ? I : 0), M0, R>>(g, task, sgrad);                      \
+            rys_thread_body<Cls<LA, LB, LC, FS, (I < FS ? I : 0), M0, R>, STAGE>(g, task, sgrad, cnr);         \
         else if constexpr (SPLIT && I < 2 * FS)                                                                 \
-            rys_thread_body<Cls<LA, LB, LC, FS, (I >= FS && I < 2 * FS ? I - FS : 0), 3, R>>(g, task, sgrad);   \
+            rys_thread_body<Cls<LA, LB, LC, FS, (I >= FS && I < 2 * FS ? I - FS : 0), 3, R>, STAGE>(g, task,   \
+                                                                                                   sgrad, cnr); \
         break;
             DFB_FSI(0) DFB_FSI(1) DFB_FSI(2) DFB_FSI(3) DFB_FSI(4) DFB_FSI(5) DFB_FSI(6) DFB_FSI(7)
             DFB_FSI(8) DFB_FSI(9) DFB_FSI(10) DFB_FSI(11) DFB_FSI(12) DFB_FSI(13) DFB_FSI(14) DFB_FSI(15)
@@ -604,6 +685,11 @@ __global__ void __launch_bounds__(128, (DFB_THREAD_MIN_BLOCKS > MINB ? DFB_THREA
         __syncthreads();
         for (int i = threadIdx.x; i < ng; i += blockDim.x)
             if (sgrad[i] != 0.0) atomicAdd(g.grad + i, sgrad[i]);
+    }
+    if constexpr (STAGE) {
+        // a copy whose wait gave up may still be landing in this block's shared memory
+        if (!staged && ((rys_smem_u32(sgrad + rys_stage_offset(ng, NR)) | (uint32_t)(uintptr_t)(g.tab.coef + g.tab.offs[NR])) & 15u) == 0)
+            if (!rys_mbar_wait(bar, 0)) atomicCAS(g.tab.err, 0, 2);
     }
 }
 

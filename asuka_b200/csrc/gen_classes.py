@@ -111,6 +111,22 @@ def plan(la, lb, lc, deriv, budget=None, f32=False):
     return None if best is None else (best[1], best[2])
 
 
+STAGE_MAX_ROOTS = 3  # tables of at most 3 roots (92 KB) fit beside 2 register-limited blocks per SM
+
+
+def staged(la, lb, lc, deriv, f32=False):
+    """Whether the class kernel copies its Rys table into shared memory (k_rys_thread STAGE).
+
+    DFB_GEN_STAGE=1 stages every eligible class (the tuner's variant build); otherwise the
+    measured table decides ("stage" for the FP64 kernels, "stage_f32" for the FP32 ones).
+    Eligible: at most STAGE_MAX_ROOTS Rys roots."""
+    if (la + lb + lc + (1 if deriv else 0)) // 2 + 1 > STAGE_MAX_ROOTS:
+        return False
+    if os.environ.get("DFB_GEN_STAGE"):
+        return os.environ["DFB_GEN_STAGE"] == "1"
+    return bool(tuning("stage_f32" if f32 else "stage").get(_key(la, lb, lc, deriv), 0))
+
+
 def tuning(field: str = "min_blocks") -> dict:
     """Per-class choices measured by asuka_b200.tune_classes ("min_blocks": launch bounds,
     "acc_budget": accumulator budget of the component split); empty when absent or when
@@ -167,10 +183,26 @@ def main() -> None:
         ]
         for (a, b, c, fs, split) in cls:
             minb = 1 if f32 else int(tune.get(_key(a, b, c, deriv), 1))
+            stage = staged(a, b, c, deriv, f32)
             kern = (f"k_rys_thread<{a}, {b}, {c}, {fs}, {'true' if deriv else 'false'}, "
-                    f"{'true' if split else 'false'}, {minb}, {'float' if f32 else 'double'}>")
+                    f"{'true' if split else 'false'}, {minb}, {'float' if f32 else 'double'}, "
+                    f"{'true' if stage else 'false'}>")
+            nr = (a + b + c + (1 if deriv else 0)) // 2 + 1
             lines.append(f"    if (lc == {c}) {{")
-            lines.append(f"        {kern}<<<dim3((unsigned)nblk, {fs * (2 if split else 1)}), 128, smem, st>>>(g);")
+            if stage:  # the Rys table after the gradient buffer and the root slots
+                lines.append(f"        const long ng = (long)(smem / sizeof(double)) - 256L * {nr};")
+                lines.append(f"        const size_t sm = sizeof(double) * (size_t)(rys_stage_offset(ng, {nr}) + "
+                             f"rys_stage_doubles(g.tab.nint, {nr}));")
+                lines.append("        static size_t attr[64];")
+                lines.append("        int dev = 0;")
+                lines.append("        cudaGetDevice(&dev);")
+                lines.append("        if (sm > attr[dev & 63]) {")
+                lines.append(f"            cudaFuncSetAttribute({kern}, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);")
+                lines.append("            attr[dev & 63] = sm;")
+                lines.append("        }")
+                lines.append(f"        {kern}<<<dim3((unsigned)nblk, {fs * (2 if split else 1)}), 128, sm, st>>>(g);")
+            else:
+                lines.append(f"        {kern}<<<dim3((unsigned)nblk, {fs * (2 if split else 1)}), 128, smem, st>>>(g);")
             lines.append("        return 1;")
             lines.append("    }")
         lines += ["    return 0;", "}", "}  // namespace dfb", ""]

@@ -1,6 +1,6 @@
 """Measured per-class kernel shapes for the class-specialised Rys kernels (the autotuner).
 
-Two knobs are tuned per angular class, each against the default build:
+Three knobs are tuned per angular class, each against the default build:
 
 * launch bounds: the thread kernels run 128 threads per block and may take up to 255
   registers (many classes use 180-230, i.e. 2 resident blocks per SM); capping them at 170
@@ -11,7 +11,10 @@ Two knobs are tuned per angular class, each against the default build:
   and recurrence tables, a larger budget (fewer, heavier threads) trades that against
   registers and parallelism (variants "acc64"/"acc96": integral budgets 64 and 96 doubles
   instead of 40; "dacc56"/"dacc72"/"dacc96"/"dacc128": derivative budgets instead of 40); a larger
-  budget also moves classes from the generic warp path onto the thread kernels.
+  budget also moves classes from the generic warp path onto the thread kernels;
+* Rys-table staging ("stage1"): classes of at most 3 roots copy their root count's coefficient
+  table into shared memory once per block (one bulk asynchronous copy) and gather from there;
+  this costs shared memory, and so occupancy, in the classes that fit several blocks per SM.
 
 Which is better is measured, not guessed.  A tuning pass covers one kind of knob (``--set``)
 and keeps the table's other entries:
@@ -59,6 +62,14 @@ VARIANTS = {
         "dacc96": dict(defines=[], gen_env={"DFB_GEN_ACC_BUDGET_DERIV": "96"}, table=("acc_budget", 96)),
         "dacc128": dict(defines=[], gen_env={"DFB_GEN_ACC_BUDGET_DERIV": "128"}, table=("acc_budget", 128)),
     },
+    # the Rys table copied into shared memory per block (classes of at most 3 roots); one variant
+    # library serves both sets: "stage" times the FP64 kernels, "f32stage" the FP32 ones
+    "stage": {
+        "stage1": dict(defines=[], gen_env={"DFB_GEN_STAGE": "1"}, table=("stage", 1)),
+    },
+    "f32stage": {
+        "stage1": dict(defines=[], gen_env={"DFB_GEN_STAGE": "1"}, table=("stage_f32", 1)),
+    },
     # the mixed-precision derivative kernels (float accumulators: budgets count floats), timed in FP32;
     # larger uniform budgets make the (f d|.) files compile for over 40 minutes each
     "f32deriv": {
@@ -67,10 +78,10 @@ VARIANTS = {
     },
 }
 # precision the classes of a set are timed in
-_PRECISION = {"f32deriv": "mixed_all"}
+_PRECISION = {"f32deriv": "mixed_all", "f32stage": "mixed_all"}
 # the table entries a set owns: (field, class-key prefix)
 _OWNS = {"launch": ("min_blocks", ""), "int": ("acc_budget", "i"), "deriv": ("acc_budget", "d"),
-         "f32deriv": ("acc_budget_f32", "d")}
+         "f32deriv": ("acc_budget_f32", "d"), "stage": ("stage", ""), "f32stage": ("stage_f32", "")}
 MIN_GAIN = 0.03
 TABLE = os.path.join(HERE, "csrc", "class_tuning.json")
 

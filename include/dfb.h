@@ -173,6 +173,14 @@ int dfb_tc_gemm(long M, long N, long K, long batch, const dfb_tc_operand_t *A, c
 int dfb_tc_error(int reset);
 
 /*
+ * Error word of the class-specialised Rys kernels on the current device: 0, or the code of the
+ * first bounded wait on a shared-memory copy of the Rys table that gave up (1: the block fell
+ * back to the global table; 2: its copy was still in flight at exit).  reset != 0 clears it.
+ * Returns a negative DFB_ERR_* code when the table is not uploaded.  No reference counterpart.
+ */
+int dfb_rys_error(int reset);
+
+/*
  * 3c adjoint of the DF gradient: out[P] = U_P Cw^T for P < nP, written (nP, nao, nao)
  * contiguous and exactly symmetric, where U_P = Cw A_P with A_P symmetric (so U_P Cw^T =
  * Cw A_P Cw^T).  U element (P, mu, j) at U[mu * sU_mu + P * sU_P + j], j < nocc; Cw is

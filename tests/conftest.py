@@ -26,3 +26,16 @@ def pytest_collection_modifyitems(config, items):
     for it in items:
         if "gpu" in it.keywords:
             it.add_marker(skip)
+
+
+@pytest.fixture(autouse=True)
+def _rys_staging_waits(request):
+    """After every GPU test: no bounded wait of the Rys kernels' table staging gave up."""
+    yield
+    if "gpu" not in request.keywords or "asuka_b200._lib" not in sys.modules:
+        return
+    lib = sys.modules["asuka_b200._lib"]
+    if getattr(lib, "_LIB", None) is None:
+        return
+    rc = lib.lib().dfb_rys_error(1)
+    assert rc <= 0, f"Rys table staging wait gave up (code {rc})"

@@ -72,6 +72,13 @@ def test_gamma_kernel_rejects_bad_arguments_without_a_gpu():
     assert L.dfb_gamma_sym(3, 0, 4, 0, 0, 0, 0, 0, None) == 0
 
 
+def test_rys_error_word_needs_the_table():
+    """dfb_rys_error reports 'not initialised' (negative) before the Rys table is uploaded."""
+    from asuka_b200 import _lib
+
+    assert _lib.lib().dfb_rys_error(0) < 0
+
+
 def test_precision_entry_points_reject_unknown_precision_without_a_gpu():
     import ctypes
 
